@@ -1,0 +1,171 @@
+/*
+ * wds_b200.h -- C ABI of the B200 batched GGA solver and implicit adjoint.
+ *
+ * The library replaces the linear-solver hooks and the per-iteration body of
+ * the reference's batched GGA route (dgga/solver.py:2922-3179,
+ * `_cudss_forward` :2630, `_cudss_factor` :2683, `_cudss_adjoint` :2653) and
+ * the GPU implicit adjoint (dgga/autodiff.py:1157-1312, `_kf_prepare` /
+ * `_kf_solve` :898-925).  A binding from the reference would call these four
+ * entry points through ctypes with plain pointers.
+ *
+ * Units are EPANET internal units (ft, cfs).  All array arguments of
+ * wds_forward / wds_adjoint are DEVICE pointers owned by the caller; the plan
+ * owns its workspace (the terminal factor and coefficients kept for the
+ * adjoint) and frees it in wds_free.  Every call is asynchronous on the given
+ * CUDA stream (cudaStream_t passed as void*; NULL = legacy default stream).
+ *
+ * Return codes: 0 ok; negative values are errors (see WDS_E_*).  Per-scenario
+ * numerical failures (non-positive pivot, non-convergence) are reported in the
+ * `info` output array, never by trapping on the device.
+ */
+#ifndef WDS_B200_H
+#define WDS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* element kinds after the host-side set-up (reference link types mapped by
+ * GGASolver.__init__, dgga/solver.py:195-216, 745-832) */
+enum {
+  WDS_KIND_PIPE = 0,      /* PIPE (H-W or C-M)                       */
+  WDS_KIND_CVPIPE = 1,    /* pipe with check valve                   */
+  WDS_KIND_TCV = 2,       /* throttle control valve                  */
+  WDS_KIND_PUMP = 3,      /* pump (curve kind in pump_type)          */
+  WDS_KIND_PRV_FIXED = 4, /* PRV with MISSING setting: fixed open/closed valve */
+  WDS_KIND_PRV = 5        /* PRV with a setting: status-machine valve */
+};
+
+/* status codes (EPANET StatusType, dgga/solver.py:1279-1281) */
+enum {
+  WDS_XHEAD = 0, WDS_TEMPCLOSED = 1, WDS_CLOSED = 2, WDS_OPEN = 3,
+  WDS_ACTIVE = 4, WDS_XFLOW = 5, WDS_XFCV = 6, WDS_XPRESSURE = 7
+};
+
+/* per-link flag bits */
+enum {
+  WDS_F_ZERO_SPEED = 1,   /* pump with speed 0: always the closed branch   */
+  WDS_F_PUMP_LIVE = 2,    /* pump with speed > 0: pumpstatus applies        */
+  WDS_F_CHP = 4,          /* constant-horsepower pump: half-step guard      */
+  WDS_F_IS_PIPE = 8       /* CVPIPE or PIPE: carries a roughness gradient   */
+};
+
+/* tank-link flag bits (tankstatus, dgga/solver.py:536-568) */
+enum {
+  WDS_TL_OVERFLOW = 1, WDS_TL_IS_PUMP = 2, WDS_TL_PUMP_IN = 4, WDS_TL_PUMP_OUT = 8
+};
+
+/* error codes */
+enum {
+  WDS_OK = 0,
+  WDS_E_ARG = -1,         /* bad argument                                  */
+  WDS_E_CUDA = -2,        /* CUDA runtime error                            */
+  WDS_E_NOMEM = -3,       /* allocation failed                             */
+  WDS_E_UNSUPPORTED = -4, /* network outside the supported element set     */
+  WDS_E_STATE = -5        /* adjoint called without a forward in implicit mode */
+};
+
+/* per-scenario info bits written by wds_forward */
+enum {
+  WDS_INFO_NOT_PD = 1,      /* a pivot of the LDL^T factor was <= 0 or not finite */
+  WDS_INFO_UNCONVERGED = 2  /* GGA loop ran out of trials                         */
+};
+
+/* Static network description (host pointers; copied by wds_plan). */
+typedef struct WdsNetwork {
+  int32_t n_nodes;               /* N                                       */
+  int32_t n_links;               /* L                                       */
+  const int8_t* node_type;       /* [N] 0 junction, otherwise fixed head    */
+  const double* elev;            /* [N] elevation (ft)                      */
+  const int32_t* link_n1;        /* [L] start node                          */
+  const int32_t* link_n2;        /* [L] end node                            */
+  const int8_t* link_kind;       /* [L] WDS_KIND_*                          */
+  const uint8_t* link_flags;     /* [L] WDS_F_* bits                        */
+  const double* km;              /* [L] minor-loss coefficient (link->Km)   */
+  const double* km_tcv;          /* [L] effective TCV coefficient           */
+  const double* q_init;          /* [L] initial flow (cfs)                  */
+  const int8_t* status0;         /* [L] initial status code                 */
+  const int8_t* pump_type;       /* [L] -1, 0 CONST_HP, 1 POWER_FUNC, 2 CUSTOM, 3 NOCURVE */
+  const double* pump_h0;         /* [L] */
+  const double* pump_r;          /* [L] */
+  const double* pump_n;          /* [L] exponent (snapped to 1 within TINY) */
+  const double* pump_speed;      /* [L] relative speed (link setting)       */
+  const double* pump_hmax;       /* [L] shut-off head used by pumpstatus    */
+  const int32_t* curve_ptr;      /* [L+1] custom-curve point ranges         */
+  const double* curve_x;         /* custom-curve flows (user units)         */
+  const double* curve_y;         /* custom-curve heads (user units)         */
+  const double* prv_hset;        /* [L] El[n2] + setting for WDS_KIND_PRV   */
+  int32_t n_tank_links;
+  const int32_t* tl_link;        /* [T] link index                          */
+  const int32_t* tl_tank;        /* [T] tank node                           */
+  const int32_t* tl_other;       /* [T] the link's other node               */
+  const double* tl_qsign;        /* [T] +1 / -1                             */
+  const double* tl_hmax;         /* [T] */
+  const double* tl_hmin;         /* [T] */
+  const uint8_t* tl_flags;       /* [T] WDS_TL_* bits                       */
+  double hexp, qexp, rqtol, htol, qtol, ucf_flow, ucf_head;
+  int32_t checkfreq, maxcheck, extra_iter;
+  const int32_t* perm;           /* [Nj] elimination order of junction rows, or NULL */
+} WdsNetwork;
+
+/* Options of one forward call. */
+typedef struct WdsForwardOpts {
+  double accuracy;               /* hacc (relerr threshold)                  */
+  int32_t max_iter;              /* trials                                   */
+  int32_t status_machine;        /* 1: batched status machine                */
+  int32_t refine;                /* refinement steps per linear solve (2)    */
+  int32_t polish_steps;          /* reduced Newton polish steps; <0: plain solve only */
+  int64_t ke_stride;             /* row stride of ke (0: one row for all)    */
+  int64_t r_stride;              /* row stride of r  (0: one row for all)    */
+} WdsForwardOpts;
+
+typedef struct WdsPlan WdsPlan;
+
+/* Symbolic analysis (ordering, elimination tree, level schedule) and device
+ * tables for one network; workspace for up to `max_batch` scenarios.
+ * Replaces GGASolver.__init__'s index build (dgga/solver.py:283-369) and
+ * symbolic.build_symbolic (dgga/symbolic.py:475-514). */
+int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out);
+
+/* Batched forward: GGA Newton loop with status machine, optional polish and
+ * terminal factorisation kept for wds_adjoint.  Replaces GGASolver.solve
+ * (dgga/solver.py:2703-3212) and ImplicitGGASolveGPU.forward's polish
+ * (dgga/autodiff.py:1172-1243).
+ *   demand, fixed_head: [B,N]; ke: [B or 1, N]; r: [B or 1, L]
+ *   head [B,N], flow [B,L], emitter [B,N], status int8 [B,L],
+ *   iters int32 [B], relerr [B], info int32 [B] (WDS_INFO_* bits). */
+int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* opts,
+                const double* demand, const double* fixed_head,
+                const double* ke, const double* r,
+                double* head, double* flow, double* emitter, int8_t* status,
+                int32_t* iters, double* relerr, int32_t* info, void* stream);
+
+/* Reduced implicit adjoint on the terminal factor of the last implicit
+ * forward (zero new factorisations).  Replaces ImplicitGGASolveGPU.backward
+ * (dgga/autodiff.py:1246-1312).  gH, gE: [B,N]; gQ: [B,L]; outputs
+ * gd, grh, gke: [B,N]; gr: [B,L] (per scenario; batch sums are the caller's). */
+int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH,
+                const double* gQ, const double* gE, double* gd, double* grh,
+                double* gke, double* gr, void* stream);
+
+/* Statistics of the plan: [Nj, nnz_L, n_levels, n_pairs, smem_bytes,
+ * n_pcv, nnz_A_lower, threads]. */
+int wds_plan_stats(const WdsPlan* plan, int64_t* out8);
+
+/* Host copy of the symbolic structure: perm [Nj], colptr [Nj+1],
+ * rowidx [nnz_L], parent [Nj], level [Nj] (any pointer may be NULL). */
+int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
+                      int32_t* rowidx, int32_t* parent, int32_t* level);
+
+/* Release the plan and its device memory. */
+int wds_free(WdsPlan* plan);
+
+/* Last error message of this thread (static storage). */
+const char* wds_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WDS_B200_H */

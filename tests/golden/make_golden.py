@@ -1,0 +1,167 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Runs only in a container where the reference package (`dgga`) sits at
+REFERENCE_ROOT (default /root/reference); the fixtures it writes are small
+.npz files that travel with the tests.  The reference imports `wntr` at module
+top for its INP parser only; that package is absent offline, so a stub with
+the imported names is placed in sys.modules (the parser is never called: the
+networks are built by wdsgpu_b200.synth and handed over field by field).
+
+For each case the fixture stores the network (every Net field), the inputs,
+and the reference outputs of
+  * GGASolver(mode="dense", dense_status_machine=...).solve(...)   (forward)
+  * implicit_solve(..., adjoint="gpu") run on CPU                  (polished
+    state and the gradients of a sum-of-squared-heads loss)
+  * for small cases, implicit_solve(..., adjoint="cpu") on mode="epanet"
+    (the EPANET-replica path with the scipy splu adjoint).
+
+Usage:  python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+
+
+def _install_wntr_stub():
+    if "wntr" in sys.modules:
+        return
+    w = types.ModuleType("wntr")
+    ep = types.ModuleType("wntr.epanet")
+    ut = types.ModuleType("wntr.epanet.util")
+    ut.FlowUnits = type("FlowUnits", (), {})
+    nw = types.ModuleType("wntr.network")
+    el = types.ModuleType("wntr.network.elements")
+    for n in ("Junction", "Reservoir", "Tank", "Pipe", "Pump", "Valve"):
+        setattr(el, n, type(n, (), {}))
+    w.epanet, ep.util, w.network, nw.elements = ep, ut, nw, el
+    sys.modules.update({"wntr": w, "wntr.epanet": ep, "wntr.epanet.util": ut,
+                        "wntr.network": nw, "wntr.network.elements": el})
+
+
+def _load_reference():
+    _install_wntr_stub()
+    sys.path.insert(0, REFERENCE_ROOT)
+    import dgga.autodiff
+    import dgga.parse
+    import dgga.solver
+    return dgga
+
+
+def pack_net(net):
+    """Net -> flat dict of arrays for np.savez (lists/meta as JSON strings)."""
+    out = {}
+    for k, v in net.as_fields().items():
+        if k in ("node_id", "link_id", "pattern_ids", "meta", "controls_raw",
+                 "rules_raw"):
+            out["net__" + k] = np.array(json.dumps(v))
+        elif k == "patterns":
+            out["net__patterns"] = np.array(json.dumps([list(map(float, p)) for p in v]))
+        else:
+            out["net__" + k] = np.asarray(v)
+    return out
+
+
+def run_case(dgga, torch, net, d, rh, ke, sensors, accuracy, status_machine,
+             with_epanet, polish_steps=3):
+    ref_net = dgga.parse.Net(**net.as_fields())
+    sd = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense",
+                               dense_status_machine=status_machine)
+    res = {}
+    D = torch.tensor(d)
+    RH = torch.tensor(rh)
+    KE = torch.tensor(ke)
+    f = sd.solve(D, RH, ke_int=KE, status_machine=status_machine,
+                 accuracy=accuracy, assemble="csr", linear_solver="dense")
+    res["fwd_head"] = f["head_ft"].numpy()
+    res["fwd_flow"] = f["flow_cfs"].numpy()
+    res["fwd_emitter"] = f["emitter_cfs"].numpy()
+    res["fwd_iters"] = f["iters"].numpy()
+    res["fwd_relerr"] = f["relerr"].numpy()
+    res["fwd_converged"] = f["converged"].numpy()
+    if "status" in f:
+        res["fwd_status"] = f["status"].numpy()
+    # implicit solve + adjoint (GPU-route algorithm, run on CPU)
+    Dg = D.clone().requires_grad_(True)
+    KEg = torch.tensor(ke[0] if ke.ndim == 2 else ke).requires_grad_(True)
+    Rg = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+    h, q, e = dgga.autodiff.implicit_solve(
+        sd, Dg, RH, ke=KEg, r_hw=Rg, accuracy=accuracy, polish_steps=polish_steps,
+        adjoint="gpu", status_machine=status_machine, assemble="csr",
+        linear_solver="dense")
+    loss = (h[:, sensors] ** 2).sum()
+    loss.backward()
+    res["imp_head"] = h.detach().numpy()
+    res["imp_flow"] = q.detach().numpy()
+    res["imp_emitter"] = e.detach().numpy()
+    res["grad_demand"] = Dg.grad.numpy()
+    res["grad_ke"] = KEg.grad.numpy()
+    res["grad_r"] = Rg.grad.numpy()
+    res["loss"] = np.array(float(loss))
+    if with_epanet:
+        se = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
+        De = D.clone().requires_grad_(True)
+        KEe = torch.tensor(ke[0] if ke.ndim == 2 else ke).requires_grad_(True)
+        Re = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+        he, qe, ee = dgga.autodiff.implicit_solve(
+            se, De, RH, ke=KEe, r_hw=Re, accuracy=accuracy, adjoint="cpu")
+        (he[:, sensors] ** 2).sum().backward()
+        res["cpu_head"] = he.detach().numpy()
+        res["cpu_flow"] = qe.detach().numpy()
+        res["cpu_grad_demand"] = De.grad.numpy()
+        res["cpu_grad_ke"] = KEe.grad.numpy()
+        res["cpu_grad_r"] = Re.grad.numpy()
+    return res
+
+
+def main():
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    cases = {}
+    # config 1: 31 junctions, plain steady GGA (no status machine needed)
+    net = synth.config1_network()
+    d0 = net.demand_cfs_at(0)
+    d = np.stack([d0 * f for f in (0.9, 1.0, 1.1)])
+    rh = np.broadcast_to(net.reservoir_head_ft_at(0), d.shape).copy()
+    ke = np.broadcast_to(net.node_ke, d.shape).copy()
+    sens = synth.sensor_nodes(net, 5)
+    cases["cfg1"] = (net, d, rh, ke, sens, 1e-9, False, True)
+    # config 2: 782 junctions, 3 PRVs, 20 emitters, status machine
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, 4, seed=11)
+    ke = np.broadcast_to(net.node_ke, d.shape).copy()
+    sens = synth.sensor_nodes(net, 30)
+    cases["cfg2"] = (net, d, rh, ke, sens, 1e-6, True, False)
+    # every element of the batched path, tank mid-range and at its bottom
+    for tag, lvl in (("feat_mid", 0.5), ("feat_low", 0.0)):
+        net = synth.feature_network(tank_level=lvl)
+        d, _ = synth.config2_scenarios(net, 6, seed=3, sigma=0.4)
+        rh = np.broadcast_to(net.fixed_head_ft_at(0), d.shape).copy()
+        ke = np.broadcast_to(net.node_ke, d.shape).copy()
+        sens = synth.sensor_nodes(net, 6)
+        cases[tag] = (net, d, rh, ke, sens, 1e-7, True, False)
+    for tag, (net, d, rh, ke, sens, acc, sm, ep) in cases.items():
+        res = run_case(dgga, torch, net, d, rh, ke, sens, acc, sm, ep)
+        blob = pack_net(net)
+        blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke,
+                     "in_sensors": np.asarray(sens), "in_accuracy": np.array(acc),
+                     "in_status_machine": np.array(sm)})
+        blob.update({"ref_" + k: v for k, v in res.items()})
+        path = os.path.join(HERE, tag + ".npz")
+        np.savez_compressed(path, **blob)
+        print("%-9s iters=%s -> %s (%d KB)" % (
+            tag, res["fwd_iters"].tolist(), os.path.basename(path),
+            os.path.getsize(path) // 1024))
+
+
+if __name__ == "__main__":
+    main()

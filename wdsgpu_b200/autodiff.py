@@ -1,0 +1,178 @@
+"""Implicit-function adjoint on the B200 route.
+
+`implicit_solve(..., adjoint="gpu")` mirrors the reference entry point
+(dgga/autodiff.py:1315-1351) and `ImplicitGGASolveSM100` mirrors
+`ImplicitGGASolveGPU` (dgga/autodiff.py:1157-1312):
+
+* forward: one `wds_forward` launch runs the GGA loop with the batched status
+  machine, `polish_steps` reduced Newton steps (Woodbury row replacement for
+  ACTIVE PRVs) and a terminal factorisation kept in the plan's workspace;
+* backward: one `wds_adjoint` launch solves the reduced node adjoint on that
+  terminal factor (zero new factorisations) and contracts it into
+  dL/d(demand, reservoir head, emitter Ke, pipe resistance).  1-D parameters
+  receive the batch-summed gradient (dgga/autodiff.py:1306-1308).
+
+Refusals follow the reference: unconverged scenarios, second derivatives,
+pump parameters, constant-HP pumps on their clamp branch, PRVs that share a
+downstream junction or cascade.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .solver import CBIG, GGASolver
+
+__all__ = ["implicit_solve", "ImplicitGGASolveSM100", "hw_resistance", "dr_dC"]
+
+
+def _adjoint_guards(s: GGASolver, flow, S):
+    if s.n_pcv:
+        j1 = s._n1[s.pcv_links]
+        j2 = s._n2[s.pcv_links]
+        if np.unique(j2).size < j2.size:
+            raise NotImplementedError(
+                "adjoint='gpu': several PRVs share one downstream junction")
+        if np.intersect1d(j2, j1).size:
+            raise NotImplementedError(
+                "adjoint='gpu': cascaded PRVs (a downstream junction is another "
+                "PRV's upstream junction)")
+    chp = s._tables["pump_type"] == 0
+    if chp.any():
+        t = s._tables
+        ks = np.flatnonzero(chp)
+        dev = flow.device
+        kt = torch.as_tensor(ks, device=dev)
+        q = flow.index_select(1, kt)
+        sgn = torch.where(q < 0, -1.0, 1.0)
+        qa = (q * sgn).clamp_min(1e-30)
+        sp = torch.as_tensor(np.maximum(t["pump_speed"][ks], 1e-12), device=dev)
+        re = torch.as_tensor(t["pump_r"][ks], device=dev) * sp ** (
+            2.0 - torch.as_tensor(t["pump_n"][ks], device=dev))
+        raw = -re / qa / qa
+        closed = (S.index_select(1, kt) <= 2) | torch.as_tensor(
+            (t["flags"][ks] & _lib.F_ZERO_SPEED) != 0, device=dev)
+        bad = ~closed & ((raw > CBIG) | (raw < s.rqtol))
+        if bool(bad.any()):
+            raise NotImplementedError(
+                "adjoint='gpu': a constant-HP pump sits on its CBIG/RQtol clamp "
+                "branch at the converged state")
+
+
+class ImplicitGGASolveSM100(torch.autograd.Function):
+    """(demand, res_head, ke, r_hw, solver, accuracy, max_iter, status_machine,
+    polish_steps) -> (head[B,N], flow[B,L], emitter[B,N])."""
+
+    @staticmethod
+    def forward(ctx, demand, res_head, ke, r_hw, solver, accuracy=1e-12,
+                max_iter=200, status_machine=None, polish_steps=3):
+        s = solver
+        dims = (demand.dim(), res_head.dim(), ke.dim(), r_hw.dim())
+        devs = (demand.device, res_head.device, ke.device, r_hw.device)
+        sm = s.dense_status_machine if status_machine is None else bool(status_machine)
+        s._guards(sm, "csr", "sm100", None, None, False)
+        d, rh, ke_t, r_t, B, _ = s._inputs(demand.detach(), res_head.detach(),
+                                           ke.detach(), r_hw.detach())
+        if ke_t.shape[0] == 1 and B > 1:
+            ke_t = ke_t.contiguous()
+        o = s.run(d, rh, ke_t, r_t, B, int(max_iter), float(accuracy), sm, int(polish_steps))
+        info = o["info"]
+        if bool((info != 0).any()):
+            bad = torch.nonzero(info != 0).flatten().tolist()
+            np_ = torch.nonzero(info & _lib.INFO_NOT_PD).flatten().tolist()
+            if np_:
+                raise RuntimeError(
+                    "adjoint='gpu': the node matrix of scenarios %s is not positive "
+                    "definite" % np_[:8])
+            raise RuntimeError(
+                "adjoint='gpu': scenarios %s did not converge (relerr=%s > accuracy=%g)"
+                % (bad[:8], [float(o["relerr"][b]) for b in bad[:4]], float(accuracy)))
+        _adjoint_guards(s, o["flow"], o["status"])
+        ctx.solver = s
+        ctx.plan = o["plan"]
+        ctx.B = B
+        ctx.dims = dims
+        ctx.devs = devs
+        ctx.L = s.L
+        head, flow, emit = o["head"], o["flow"], o["emit"]
+        if all(x == 1 for x in dims[:3]):
+            head, flow, emit = head[0], flow[0], emit[0]
+        return head, flow, emit
+
+    @staticmethod
+    def backward(ctx, gH, gQ, gE):
+        if torch.is_grad_enabled():
+            raise NotImplementedError(
+                "adjoint='gpu' is first order only (create_graph / second "
+                "derivatives are not supported)")
+        s = ctx.solver
+        B, dev = ctx.B, s.device
+        N, L = s.N, s.L
+
+        def _g(g, n):
+            if g is None:
+                return torch.zeros(B, n, dtype=torch.float64, device=dev)
+            g = g.detach().to(dtype=torch.float64, device=dev)
+            g = g.unsqueeze(0).expand(B, -1) if g.dim() == 1 else g
+            return g.contiguous()
+
+        gH, gQ, gE = _g(gH, N), _g(gQ, L), _g(gE, N)
+        gd = torch.empty(B, N, dtype=torch.float64, device=dev)
+        grh = torch.empty_like(gd)
+        gke = torch.empty_like(gd)
+        gr = torch.empty(B, L, dtype=torch.float64, device=dev)
+        p = ctx.plan
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        import ctypes
+        _lib.check(p.lib.wds_adjoint(
+            p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
+            grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(stream)),
+            "wds_adjoint")
+        dm, dv = ctx.dims, ctx.devs
+
+        def _fit(g, dim, d_):
+            g = g.to(device=d_)
+            return g.sum(0) if dim == 1 else g
+
+        return (_fit(gd, dm[0], dv[0]), _fit(grh, dm[1], dv[1]), _fit(gke, dm[2], dv[2]),
+                _fit(gr, dm[3] + 1, dv[3]), None, None, None, None, None)
+
+
+def implicit_solve(solver, demand, res_head, ke=None, r_hw=None, accuracy=1e-12,
+                   max_iter=200, polish_steps=3, speed=None, pump_h0=None, pump_r=None,
+                   status=None, adjoint="gpu", status_machine=None, assemble="csr",
+                   linear_solver="sm100"):
+    """Forward + implicit adjoint (dgga/autodiff.py:1315-1351 contract).
+    Returns (head, flow, emitter); differentiable w.r.t. demand, res_head, ke
+    and r_hw."""
+    if adjoint == "cpu":
+        raise NotImplementedError(
+            "adjoint='cpu' is the reference's scipy splu adjoint; this package "
+            "provides adjoint='gpu'")
+    if adjoint != "gpu":
+        raise ValueError("adjoint must be 'cpu'/'gpu', got %r" % (adjoint,))
+    if speed is not None or pump_h0 is not None or pump_r is not None or status is not None:
+        raise NotImplementedError(
+            "adjoint='gpu' takes no speed/pump_h0/pump_r/status (pump parameter "
+            "gradients are CPU-adjoint only in the reference)")
+    if assemble != "csr" or linear_solver != "sm100":
+        raise ValueError("the B200 route is assemble='csr', linear_solver='sm100'")
+    dev = solver.device
+    t = lambda x: x.to(dtype=torch.float64, device=dev) if isinstance(x, torch.Tensor) \
+        else torch.as_tensor(np.asarray(x), dtype=torch.float64, device=dev)
+    ke = solver.node_ke_default if ke is None else ke
+    r_hw = solver.r_hw if r_hw is None else r_hw
+    return ImplicitGGASolveSM100.apply(t(demand), t(res_head), t(ke), t(r_hw), solver,
+                                       accuracy, max_iter, status_machine, int(polish_steps))
+
+
+# Roughness chain rule (dgga/calib.py:64-89): r = 4.727 L / C^1.852 / D^4.871.
+def hw_resistance(C, length_ft, diam_ft):
+    """Hazen-Williams resistance of pipes with roughness C (internal units)."""
+    return 4.727 * length_ft / C ** 1.852 / diam_ft ** 4.871
+
+
+def dr_dC(C, length_ft, diam_ft):
+    """d r / d C = -1.852 r / C."""
+    return -1.852 * hw_resistance(C, length_ft, diam_ft) / C

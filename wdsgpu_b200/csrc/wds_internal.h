@@ -1,0 +1,148 @@
+// Internal layout shared by the host planner (wds_plan.cu) and the kernels
+// (wds_kernels.cu).  Not part of the public ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "wds_b200.h"
+
+namespace wds {
+
+constexpr double kCSMALL = 1e-6;   // hydcoeffs.c CSMALL, dgga/solver.py:34
+constexpr double kCBIG = 1e8;      // dgga/solver.py:35
+constexpr double kBIG = 1e10;
+constexpr double kQZERO = 1e-6;
+
+// Device tables of one network.  Junction vectors are indexed by their
+// elimination index p (0..Nj-1); link ends are "end codes": p >= 0 for a
+// junction, -(f+1) for the f-th fixed-head node.
+struct DevNet {
+  int N, L, Nj, Nf, nnzL, nlev, npcv, ntl, npairs, nfill, nxf, nftask, nfpair;
+  // links [L]
+  const int* e1;
+  const int* e2;
+  const int8_t* kind;
+  const uint8_t* flags;
+  const int8_t* status0;
+  const int8_t* ptype;
+  const double* km;
+  const double* km_tcv;
+  const double* q_init;
+  const double* ph0;
+  const double* pr;
+  const double* pn;
+  const double* pspeed;
+  const double* phmax;
+  const int* cptr;        // [L+1]
+  const double* cx;
+  const double* cy;
+  const int* link_tl;     // [L] tank-link index or -1
+  const int* link_pcv;    // [L] pcv index or -1
+  // junctions, elimination order [Nj]
+  const int* jnode;       // node index
+  const double* el;       // elevation
+  const int* inc_ptr;     // [Nj+1]
+  const int* inc_split;   // [Nj] first n2-side entry
+  const int* inc;         // link index of each incidence entry
+  const int* node_xf;     // [Nj] Xflow save slot or -1
+  const int* cb_ptr;      // [Nj+1] pcv valves whose downstream node is p
+  const int* cb_idx;
+  // fixed nodes [Nf]
+  const int* fnode;
+  const int* finc_ptr;    // [Nf+1]
+  const int* finc_split;  // [Nf]
+  const int* finc;
+  // off-diagonal entries of A
+  const int* pair_ptr;    // [npairs+1]
+  const int* pair_link;
+  const int* pair_slot;   // [npairs]
+  const int* fill_slot;   // [nfill]
+  // symbolic structure of L (column-major, diagonal first)
+  const int* colptr;      // [Nj+1]
+  const int* rowidx;      // [nnzL]
+  const int* levptr;      // [nlev+1]
+  const int* levcol;      // [Nj]
+  const int* ftask_ptr;   // [nlev+1]
+  const int4* ftask;      // {slot, pair_begin, pair_end, is_diag}
+  const int* fpair;       // [3*nfpair] {s1, s2, diag slot of k}
+  const int* rptr;        // [Nj+1] row lists (forward solve)
+  const int* rslot;
+  const int* rcol;
+  // status-machine PRVs [npcv]
+  const int* pcv_link;
+  const int* pcv_j1;
+  const int* pcv_j2;
+  const int* pcv_off;     // slot of (j1,j2)
+  const int* pcv_xf;      // Xflow slot of j2
+  const double* pcv_hset;
+  const double* pcv_km;
+  // tank links [ntl]
+  const int* tl_link;
+  const int* tl_tank;     // fixed index
+  const int* tl_other;    // end code
+  const double* tl_qsign;
+  const double* tl_hmax;
+  const double* tl_hmin;
+  const uint8_t* tl_flags;
+  double hexp, qexp, rqtol, htol, qtol, ucf_flow, ucf_head;
+  int checkfreq, maxcheck, extra_iter;
+};
+
+// Workspace kept between the forward (implicit mode) and the adjoint.
+struct DevWork {
+  double* W;      // [B][nnzL] terminal factor (unscaled columns, 1/D on diagonal)
+  double* P;      // [B][L]
+  double* dr;     // [B][L]
+  double* emh;    // [B][Nj]
+  double* hge;    // [B][Nj]
+  double* dke;    // [B][Nj]
+  int8_t* act;    // [B][max(npcv,1)]
+  double* scr;    // [B][nscr][Nj] scratch vectors
+  int nscr;
+  int* valid;     // [B] 1 when the terminal state is stored
+};
+
+struct FwdArgs {
+  int B;
+  double hacc;
+  int max_iter, sm, refine, polish;
+  long long ke_stride, r_stride;
+  const double* d;
+  const double* rh;
+  const double* ke;
+  const double* r;
+  double* head;
+  double* flow;
+  double* emit;
+  int8_t* status;
+  int* iters;
+  double* relerr;
+  int* info;
+};
+
+struct AdjArgs {
+  int B;
+  const double* gH;
+  const double* gQ;
+  const double* gE;
+  double* gd;
+  double* grh;
+  double* gke;
+  double* gr;
+};
+
+// Host-side symbolic data kept in the plan (for inspection and tests).
+struct HostSym {
+  int Nj = 0;
+  std::vector<int> perm, iperm, parent, level, colptr, rowidx;
+};
+
+int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a,
+                   size_t smem, int threads, void* stream, std::string* err);
+int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a,
+                   size_t smem, int threads, void* stream, std::string* err);
+size_t forward_smem_bytes(const DevNet& n, int threads);
+size_t adjoint_smem_bytes(const DevNet& n, int threads);
+
+}  // namespace wds

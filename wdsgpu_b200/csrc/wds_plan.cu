@@ -1,0 +1,552 @@
+// Host planner: symbolic analysis of the junction graph and the device tables
+// of one network (replaces GGASolver.__init__'s index build,
+// dgga/solver.py:239-369, and symbolic.build_symbolic, dgga/symbolic.py:475).
+//
+//  * ordering: minimum degree on the elimination graph (ties broken by the
+//    smallest junction row), or a caller-supplied permutation;
+//  * elimination tree and the structure of L by merging children's column
+//    structures; columns scheduled by elimination-tree level (leaves first);
+//  * left-looking LDL^T task lists: one task per entry of L, each a list of
+//    (L_ik, L_jk, 1/D_k) update triples in ascending k;
+//  * deterministic gather maps for the assembly (per-junction incidence lists
+//    in the reference's scatter order, per-pair link lists).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "wds_internal.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+// Minimum-degree ordering on the explicit elimination graph.
+std::vector<int> min_degree(int n, std::vector<std::vector<int>> adj) {
+  std::vector<int> deg(n), order;
+  order.reserve(n);
+  std::vector<char> alive(n, 1);
+  std::set<std::pair<int, int>> pq;
+  for (int i = 0; i < n; ++i) {
+    deg[i] = (int)adj[i].size();
+    pq.insert({deg[i], i});
+  }
+  std::vector<int> merged;
+  while (!pq.empty()) {
+    int v = pq.begin()->second;
+    pq.erase(pq.begin());
+    alive[v] = 0;
+    order.push_back(v);
+    std::vector<int> nb;
+    for (int u : adj[v])
+      if (alive[u]) nb.push_back(u);
+    for (int u : nb) {
+      pq.erase({deg[u], u});
+      merged.clear();
+      std::set_union(adj[u].begin(), adj[u].end(), nb.begin(), nb.end(),
+                     std::back_inserter(merged));
+      std::vector<int> nu;
+      nu.reserve(merged.size());
+      for (int w : merged)
+        if (w != u && alive[w]) nu.push_back(w);
+      adj[u].swap(nu);
+      deg[u] = (int)adj[u].size();
+      pq.insert({deg[u], u});
+    }
+    adj[v].clear();
+  }
+  return order;
+}
+
+struct Blob {
+  std::vector<unsigned char> bytes;
+  template <class T>
+  size_t add(const std::vector<T>& v) {
+    size_t off = (bytes.size() + 255) / 256 * 256;
+    bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 1));
+    if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+  }
+};
+
+}  // namespace
+
+struct WdsPlan {
+  wds::DevNet dn{};
+  wds::DevWork dw{};
+  wds::HostSym sym;
+  void* dtab = nullptr;
+  void* dwork = nullptr;
+  int max_batch = 0;
+  int threads = 256;
+  size_t smem_fwd = 0, smem_adj = 0;
+  int nnzA_lower = 0;
+  bool have_state = false;
+  int state_batch = 0;
+};
+
+extern "C" const char* wds_last_error(void) { return g_err.c_str(); }
+
+extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out) {
+  using namespace wds;
+  if (!net || !out || max_batch <= 0) return fail(WDS_E_ARG, "wds_plan: bad argument");
+  *out = nullptr;
+  const int N = net->n_nodes, L = net->n_links;
+  if (N <= 0 || L <= 0) return fail(WDS_E_ARG, "wds_plan: empty network");
+  // ---- junction rows (file order) and fixed nodes
+  std::vector<int> jrow(N, -1), jnodes, fix_idx(N, -1), fnodes;
+  for (int i = 0; i < N; ++i) {
+    if (net->node_type[i] == 0) {
+      jrow[i] = (int)jnodes.size();
+      jnodes.push_back(i);
+    } else {
+      fix_idx[i] = (int)fnodes.size();
+      fnodes.push_back(i);
+    }
+  }
+  const int Nj = (int)jnodes.size(), Nf = (int)fnodes.size();
+  if (Nj == 0) return fail(WDS_E_ARG, "wds_plan: no junctions");
+  for (int k = 0; k < L; ++k) {
+    int a = net->link_n1[k], b = net->link_n2[k];
+    if (a < 0 || a >= N || b < 0 || b >= N)
+      return fail(WDS_E_ARG, "wds_plan: link end out of range");
+    int kd = net->link_kind[k];
+    if (kd < WDS_KIND_PIPE || kd > WDS_KIND_PRV)
+      return fail(WDS_E_UNSUPPORTED, "wds_plan: unsupported link kind");
+  }
+  // ---- junction graph
+  std::vector<std::vector<int>> adj(Nj);
+  for (int k = 0; k < L; ++k) {
+    int a = jrow[net->link_n1[k]], b = jrow[net->link_n2[k]];
+    if (a >= 0 && b >= 0 && a != b) {
+      adj[a].push_back(b);
+      adj[b].push_back(a);
+    }
+  }
+  for (auto& v : adj) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  // ---- ordering
+  std::vector<int> perm(Nj), iperm(Nj);
+  if (net->perm) {
+    std::vector<char> seen(Nj, 0);
+    for (int p = 0; p < Nj; ++p) {
+      int r = net->perm[p];
+      if (r < 0 || r >= Nj || seen[r]) return fail(WDS_E_ARG, "wds_plan: perm is not a permutation");
+      seen[r] = 1;
+      perm[p] = r;
+    }
+  } else {
+    perm = min_degree(Nj, adj);
+  }
+  for (int p = 0; p < Nj; ++p) iperm[perm[p]] = p;
+  // ---- symbolic factorisation: struct(L_j) = A_{>j,j} U children \ {j}
+  std::vector<std::vector<int>> cstruct(Nj), children(Nj);
+  std::vector<int> parent(Nj, -1), level(Nj, 0), mark(Nj, -1);
+  for (int j = 0; j < Nj; ++j) {
+    std::vector<int>& s = cstruct[j];
+    mark[j] = j;
+    for (int u : adj[perm[j]]) {
+      int i = iperm[u];
+      if (i > j && mark[i] != j) {
+        mark[i] = j;
+        s.push_back(i);
+      }
+    }
+    int lv = 0;
+    for (int c : children[j]) {
+      lv = std::max(lv, level[c] + 1);
+      for (int i : cstruct[c])
+        if (i != j && mark[i] != j) {
+          mark[i] = j;
+          s.push_back(i);
+        }
+    }
+    level[j] = lv;
+    std::sort(s.begin(), s.end());
+    if (!s.empty()) {
+      parent[j] = s[0];
+      children[s[0]].push_back(j);
+    }
+  }
+  std::vector<int> colptr(Nj + 1, 0), rowidx;
+  for (int j = 0; j < Nj; ++j) colptr[j + 1] = colptr[j] + 1 + (int)cstruct[j].size();
+  const int nnzL = colptr[Nj];
+  rowidx.resize(nnzL);
+  for (int j = 0; j < Nj; ++j) {
+    rowidx[colptr[j]] = j;
+    for (size_t t = 0; t < cstruct[j].size(); ++t) rowidx[colptr[j] + 1 + t] = cstruct[j][t];
+  }
+  auto slot = [&](int i, int j) -> int {  // i >= j
+    if (i == j) return colptr[j];
+    auto b = rowidx.begin() + colptr[j] + 1, e = rowidx.begin() + colptr[j + 1];
+    auto it = std::lower_bound(b, e, i);
+    if (it == e || *it != i) return -1;
+    return (int)(it - rowidx.begin());
+  };
+  int nlev = 0;
+  for (int j = 0; j < Nj; ++j) nlev = std::max(nlev, level[j] + 1);
+  std::vector<int> levptr(nlev + 1, 0), levcol;
+  for (int j = 0; j < Nj; ++j) levptr[level[j] + 1]++;
+  for (int l = 0; l < nlev; ++l) levptr[l + 1] += levptr[l];
+  levcol.resize(Nj);
+  {
+    std::vector<int> pos(levptr.begin(), levptr.end() - 1);
+    for (int j = 0; j < Nj; ++j) levcol[pos[level[j]]++] = j;
+  }
+  // row lists: rows[i] = { k < i : i in struct(k) } ascending
+  std::vector<std::vector<int>> rows(Nj);
+  for (int k = 0; k < Nj; ++k)
+    for (int i : cstruct[k]) rows[i].push_back(k);
+  std::vector<int> rptr(Nj + 1, 0), rslot, rcol;
+  for (int j = 0; j < Nj; ++j) {
+    for (int k : rows[j]) {
+      rslot.push_back(slot(j, k));
+      rcol.push_back(k);
+    }
+    rptr[j + 1] = (int)rcol.size();
+  }
+  // factor tasks by level
+  std::vector<int> ftask_ptr(nlev + 1, 0), fpair;
+  std::vector<int4> ftask;
+  for (int l = 0; l < nlev; ++l) {
+    for (int t = levptr[l]; t < levptr[l + 1]; ++t) {
+      int j = levcol[t];
+      for (int e = colptr[j]; e < colptr[j + 1]; ++e) {
+        int i = rowidx[e];
+        int pb = (int)fpair.size() / 3;
+        for (int k : rows[j]) {
+          int sik = slot(i, k);
+          if (sik < 0) continue;
+          fpair.push_back(sik);
+          fpair.push_back(slot(j, k));
+          fpair.push_back(colptr[k]);
+        }
+        int pe = (int)fpair.size() / 3;
+        ftask.push_back(make_int4(e, pb, pe, i == j ? 1 : 0));
+      }
+    }
+    ftask_ptr[l + 1] = (int)ftask.size();
+  }
+  // ---- link end codes, incidence lists, pairs
+  auto code = [&](int nd) { return jrow[nd] >= 0 ? iperm[jrow[nd]] : -(fix_idx[nd] + 1); };
+  std::vector<int> e1(L), e2(L);
+  for (int k = 0; k < L; ++k) {
+    e1[k] = code(net->link_n1[k]);
+    e2[k] = code(net->link_n2[k]);
+  }
+  std::vector<std::vector<int>> inc1(Nj), inc2(Nj), finc1(Nf), finc2(Nf);
+  for (int k = 0; k < L; ++k) {
+    if (e1[k] >= 0) inc1[e1[k]].push_back(k); else finc1[-e1[k] - 1].push_back(k);
+    if (e2[k] >= 0) inc2[e2[k]].push_back(k); else finc2[-e2[k] - 1].push_back(k);
+  }
+  std::vector<int> inc_ptr(Nj + 1, 0), inc_split(Nj), inc;
+  for (int p = 0; p < Nj; ++p) {
+    inc.insert(inc.end(), inc1[p].begin(), inc1[p].end());
+    inc_split[p] = (int)inc.size();
+    inc.insert(inc.end(), inc2[p].begin(), inc2[p].end());
+    inc_ptr[p + 1] = (int)inc.size();
+  }
+  std::vector<int> finc_ptr(Nf + 1, 0), finc_split(std::max(Nf, 1), 0), finc;
+  for (int f = 0; f < Nf; ++f) {
+    finc.insert(finc.end(), finc1[f].begin(), finc1[f].end());
+    finc_split[f] = (int)finc.size();
+    finc.insert(finc.end(), finc2[f].begin(), finc2[f].end());
+    finc_ptr[f + 1] = (int)finc.size();
+  }
+  std::map<std::pair<int, int>, std::vector<int>> pairs;
+  for (int k = 0; k < L; ++k)
+    if (e1[k] >= 0 && e2[k] >= 0 && e1[k] != e2[k])
+      pairs[{std::max(e1[k], e2[k]), std::min(e1[k], e2[k])}].push_back(k);
+  std::vector<int> pair_ptr(1, 0), pair_link, pair_slot;
+  std::vector<char> is_a(nnzL, 0);
+  std::map<std::pair<int, int>, int> pair_slot_of;
+  for (auto& kv : pairs) {
+    int s = slot(kv.first.first, kv.first.second);
+    if (s < 0) return fail(WDS_E_ARG, "wds_plan: internal error (pair outside pattern)");
+    is_a[s] = 1;
+    pair_slot_of[kv.first] = s;
+    pair_slot.push_back(s);
+    pair_link.insert(pair_link.end(), kv.second.begin(), kv.second.end());
+    pair_ptr.push_back((int)pair_link.size());
+  }
+  std::vector<int> fill_slot;
+  for (int j = 0; j < Nj; ++j)
+    for (int e = colptr[j] + 1; e < colptr[j + 1]; ++e)
+      if (!is_a[e]) fill_slot.push_back(e);
+  // ---- status-machine PRVs
+  std::vector<int> link_pcv(L, -1), pcv_link, pcv_j1, pcv_j2, pcv_off, pcv_xf, node_xf(Nj, -1);
+  std::vector<double> pcv_hset, pcv_km;
+  int nxf = 0;
+  for (int k = 0; k < L; ++k) {
+    if (net->link_kind[k] != WDS_KIND_PRV) continue;
+    if (e1[k] < 0 || e2[k] < 0)
+      return fail(WDS_E_UNSUPPORTED, "wds_plan: a PRV with a setting must join two junctions");
+    link_pcv[k] = (int)pcv_link.size();
+    pcv_link.push_back(k);
+    pcv_j1.push_back(e1[k]);
+    pcv_j2.push_back(e2[k]);
+    pcv_off.push_back(pair_slot_of[{std::max(e1[k], e2[k]), std::min(e1[k], e2[k])}]);
+    if (node_xf[e2[k]] < 0) node_xf[e2[k]] = nxf++;
+    pcv_xf.push_back(node_xf[e2[k]]);
+    pcv_hset.push_back(net->prv_hset[k]);
+    pcv_km.push_back(net->km[k]);
+  }
+  const int npcv = (int)pcv_link.size();
+  std::vector<int> cb_ptr(Nj + 1, 0), cb_idx;
+  {
+    std::vector<std::vector<int>> cb(Nj);
+    for (int i = 0; i < npcv; ++i) cb[pcv_j2[i]].push_back(i);
+    for (int p = 0; p < Nj; ++p) {
+      cb_idx.insert(cb_idx.end(), cb[p].begin(), cb[p].end());
+      cb_ptr[p + 1] = (int)cb_idx.size();
+    }
+  }
+  // ---- tank links
+  const int ntl = net->n_tank_links;
+  std::vector<int> link_tl(L, -1), tl_link(ntl), tl_tank(ntl), tl_other(ntl);
+  std::vector<double> tl_qsign(ntl), tl_hmax(ntl), tl_hmin(ntl);
+  std::vector<uint8_t> tl_flags(ntl);
+  for (int t = 0; t < ntl; ++t) {
+    int k = net->tl_link[t];
+    if (k < 0 || k >= L || fix_idx[net->tl_tank[t]] < 0)
+      return fail(WDS_E_ARG, "wds_plan: bad tank link");
+    link_tl[k] = t;
+    tl_link[t] = k;
+    tl_tank[t] = fix_idx[net->tl_tank[t]];
+    tl_other[t] = code(net->tl_other[t]);
+    tl_qsign[t] = net->tl_qsign[t];
+    tl_hmax[t] = net->tl_hmax[t];
+    tl_hmin[t] = net->tl_hmin[t];
+    tl_flags[t] = net->tl_flags[t];
+  }
+  // ---- per-link copies
+  std::vector<int8_t> kind(net->link_kind, net->link_kind + L),
+      st0(net->status0, net->status0 + L), ptype(net->pump_type, net->pump_type + L);
+  std::vector<uint8_t> flags(net->link_flags, net->link_flags + L);
+  std::vector<double> km(net->km, net->km + L), km_tcv(net->km_tcv, net->km_tcv + L),
+      q_init(net->q_init, net->q_init + L), ph0(net->pump_h0, net->pump_h0 + L),
+      pr(net->pump_r, net->pump_r + L), pn(net->pump_n, net->pump_n + L),
+      psp(net->pump_speed, net->pump_speed + L), phm(net->pump_hmax, net->pump_hmax + L);
+  std::vector<int> cptr(net->curve_ptr, net->curve_ptr + L + 1);
+  std::vector<double> cx(net->curve_x, net->curve_x + cptr[L]), cy(net->curve_y, net->curve_y + cptr[L]);
+  std::vector<double> el(Nj);
+  std::vector<int> jn(Nj);
+  for (int p = 0; p < Nj; ++p) {
+    jn[p] = jnodes[perm[p]];
+    el[p] = net->elev[jn[p]];
+  }
+  // ---- bounds check of every index the kernels dereference (host side, so
+  // that a table error is an error return and never a device fault)
+  {
+    auto in = [](int v, int lo, int hi) { return v >= lo && v < hi; };
+    auto endok = [&](int c) { return c >= 0 ? c < Nj : (-c - 1) < Nf; };
+    bool ok = true;
+    for (int k = 0; k < L && ok; ++k) ok = endok(e1[k]) && endok(e2[k]);
+    for (int v : inc) ok = ok && in(v, 0, L);
+    for (int v : finc) ok = ok && in(v, 0, L);
+    for (int v : pair_link) ok = ok && in(v, 0, L);
+    for (int v : pair_slot) ok = ok && in(v, 0, nnzL);
+    for (int v : fill_slot) ok = ok && in(v, 0, nnzL);
+    for (int v : rowidx) ok = ok && in(v, 0, Nj);
+    for (int v : levcol) ok = ok && in(v, 0, Nj);
+    for (int v : fpair) ok = ok && in(v, 0, nnzL);
+    for (auto& t : ftask) ok = ok && in(t.x, 0, nnzL) && t.y >= 0 && t.y <= t.z &&
+                             t.z <= (int)fpair.size() / 3;
+    for (int v : rslot) ok = ok && in(v, 0, nnzL);
+    for (int v : rcol) ok = ok && in(v, 0, Nj);
+    for (int v : cb_idx) ok = ok && in(v, 0, std::max(npcv, 1));
+    for (int i = 0; i < npcv; ++i)
+      ok = ok && in(pcv_j1[i], 0, Nj) && in(pcv_j2[i], 0, Nj) && in(pcv_off[i], 0, nnzL) &&
+           in(pcv_xf[i], 0, std::max(nxf, 1)) && in(pcv_link[i], 0, L);
+    for (int p = 0; p < Nj; ++p) ok = ok && node_xf[p] < std::max(nxf, 1);
+    for (int t = 0; t < ntl; ++t) ok = ok && in(tl_tank[t], 0, Nf) && endok(tl_other[t]);
+    for (int k = 0; k < L; ++k) {
+      if (net->pump_type[k] == 2 && net->link_kind[k] == WDS_KIND_PUMP)
+        ok = ok && net->curve_ptr[k + 1] - net->curve_ptr[k] >= 2;
+      ok = ok && net->curve_ptr[k] <= net->curve_ptr[k + 1];
+    }
+    for (int p = 0; p < Nj; ++p) ok = ok && in(jn[p], 0, N);
+    for (int f = 0; f < Nf; ++f) ok = ok && in(fnodes[f], 0, N);
+    if (!ok) return fail(WDS_E_ARG, "wds_plan: internal table failed its bounds check");
+  }
+  // ---- upload
+  Blob blob;
+  size_t o_e1 = blob.add(e1), o_e2 = blob.add(e2), o_kind = blob.add(kind), o_flags = blob.add(flags),
+         o_st0 = blob.add(st0), o_ptype = blob.add(ptype), o_km = blob.add(km),
+         o_kmt = blob.add(km_tcv), o_q0 = blob.add(q_init), o_ph0 = blob.add(ph0),
+         o_pr = blob.add(pr), o_pn = blob.add(pn), o_psp = blob.add(psp), o_phm = blob.add(phm),
+         o_cptr = blob.add(cptr), o_cx = blob.add(cx), o_cy = blob.add(cy),
+         o_ltl = blob.add(link_tl), o_lpcv = blob.add(link_pcv), o_jn = blob.add(jn),
+         o_el = blob.add(el), o_incp = blob.add(inc_ptr), o_incs = blob.add(inc_split),
+         o_inc = blob.add(inc), o_nxf = blob.add(node_xf), o_cbp = blob.add(cb_ptr),
+         o_cbi = blob.add(cb_idx), o_fn = blob.add(fnodes), o_fincp = blob.add(finc_ptr),
+         o_fincs = blob.add(finc_split), o_finc = blob.add(finc), o_pp = blob.add(pair_ptr),
+         o_pl = blob.add(pair_link), o_ps = blob.add(pair_slot), o_fs = blob.add(fill_slot),
+         o_cp = blob.add(colptr), o_ri = blob.add(rowidx), o_lp = blob.add(levptr),
+         o_lc = blob.add(levcol), o_ftp = blob.add(ftask_ptr), o_ft = blob.add(ftask),
+         o_fp = blob.add(fpair), o_rp = blob.add(rptr), o_rs = blob.add(rslot), o_rc = blob.add(rcol),
+         o_pcl = blob.add(pcv_link), o_pj1 = blob.add(pcv_j1), o_pj2 = blob.add(pcv_j2),
+         o_poff = blob.add(pcv_off), o_pxf = blob.add(pcv_xf), o_phs = blob.add(pcv_hset),
+         o_pkm = blob.add(pcv_km), o_tll = blob.add(tl_link), o_tlt = blob.add(tl_tank),
+         o_tlo = blob.add(tl_other), o_tlq = blob.add(tl_qsign), o_tlx = blob.add(tl_hmax),
+         o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags);
+  WdsPlan* plan = new WdsPlan();
+  if (cudaMalloc(&plan->dtab, blob.bytes.size()) != cudaSuccess) {
+    delete plan;
+    return fail(WDS_E_NOMEM, "wds_plan: cudaMalloc of the device tables failed");
+  }
+  if (cudaMemcpy(plan->dtab, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    cudaFree(plan->dtab);
+    delete plan;
+    return fail(WDS_E_CUDA, "wds_plan: upload of the device tables failed");
+  }
+  unsigned char* base = (unsigned char*)plan->dtab;
+#define P_(T, off) reinterpret_cast<const T*>(base + (off))
+  DevNet& d = plan->dn;
+  d.N = N; d.L = L; d.Nj = Nj; d.Nf = Nf; d.nnzL = nnzL; d.nlev = nlev; d.npcv = npcv;
+  d.ntl = ntl; d.npairs = (int)pair_slot.size(); d.nfill = (int)fill_slot.size(); d.nxf = nxf;
+  d.nftask = (int)ftask.size(); d.nfpair = (int)fpair.size() / 3;
+  d.e1 = P_(int, o_e1); d.e2 = P_(int, o_e2); d.kind = P_(int8_t, o_kind);
+  d.flags = P_(uint8_t, o_flags); d.status0 = P_(int8_t, o_st0); d.ptype = P_(int8_t, o_ptype);
+  d.km = P_(double, o_km); d.km_tcv = P_(double, o_kmt); d.q_init = P_(double, o_q0);
+  d.ph0 = P_(double, o_ph0); d.pr = P_(double, o_pr); d.pn = P_(double, o_pn);
+  d.pspeed = P_(double, o_psp); d.phmax = P_(double, o_phm); d.cptr = P_(int, o_cptr);
+  d.cx = P_(double, o_cx); d.cy = P_(double, o_cy); d.link_tl = P_(int, o_ltl);
+  d.link_pcv = P_(int, o_lpcv); d.jnode = P_(int, o_jn); d.el = P_(double, o_el);
+  d.inc_ptr = P_(int, o_incp); d.inc_split = P_(int, o_incs); d.inc = P_(int, o_inc);
+  d.node_xf = P_(int, o_nxf); d.cb_ptr = P_(int, o_cbp); d.cb_idx = P_(int, o_cbi);
+  d.fnode = P_(int, o_fn); d.finc_ptr = P_(int, o_fincp); d.finc_split = P_(int, o_fincs);
+  d.finc = P_(int, o_finc); d.pair_ptr = P_(int, o_pp); d.pair_link = P_(int, o_pl);
+  d.pair_slot = P_(int, o_ps); d.fill_slot = P_(int, o_fs); d.colptr = P_(int, o_cp);
+  d.rowidx = P_(int, o_ri); d.levptr = P_(int, o_lp); d.levcol = P_(int, o_lc);
+  d.ftask_ptr = P_(int, o_ftp); d.ftask = P_(int4, o_ft); d.fpair = P_(int, o_fp);
+  d.rptr = P_(int, o_rp); d.rslot = P_(int, o_rs); d.rcol = P_(int, o_rc);
+  d.pcv_link = P_(int, o_pcl); d.pcv_j1 = P_(int, o_pj1); d.pcv_j2 = P_(int, o_pj2);
+  d.pcv_off = P_(int, o_poff); d.pcv_xf = P_(int, o_pxf); d.pcv_hset = P_(double, o_phs);
+  d.pcv_km = P_(double, o_pkm); d.tl_link = P_(int, o_tll); d.tl_tank = P_(int, o_tlt);
+  d.tl_other = P_(int, o_tlo); d.tl_qsign = P_(double, o_tlq); d.tl_hmax = P_(double, o_tlx);
+  d.tl_hmin = P_(double, o_tln); d.tl_flags = P_(uint8_t, o_tlf);
+#undef P_
+  d.hexp = net->hexp; d.qexp = net->qexp; d.rqtol = net->rqtol; d.htol = net->htol;
+  d.qtol = net->qtol; d.ucf_flow = net->ucf_flow; d.ucf_head = net->ucf_head;
+  d.checkfreq = net->checkfreq; d.maxcheck = net->maxcheck; d.extra_iter = net->extra_iter;
+  plan->nnzA_lower = Nj + (int)pair_slot.size();
+  plan->threads = 256;
+  plan->smem_fwd = forward_smem_bytes(d, plan->threads);
+  plan->smem_adj = adjoint_smem_bytes(d, plan->threads);
+  if (plan->smem_fwd > 227 * 1024 || plan->smem_adj > 227 * 1024) {
+    cudaFree(plan->dtab);
+    delete plan;
+    return fail(WDS_E_UNSUPPORTED,
+                "wds_plan: the network's per-scenario state exceeds shared memory");
+  }
+  // ---- workspace
+  plan->max_batch = max_batch;
+  DevWork& w = plan->dw;
+  w.nscr = 4 + 2 * std::max(npcv, 1);  // heads, rp, res, sx, 2p Woodbury columns
+  const size_t B = (size_t)max_batch, pc = (size_t)std::max(npcv, 1);
+  size_t bytes = 0;
+  auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
+  size_t ow = take(B * nnzL * 8), op = take(B * L * 8), odr = take(B * L * 8),
+         oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
+         oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4);
+  if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
+    cudaFree(plan->dtab);
+    delete plan;
+    return fail(WDS_E_NOMEM, "wds_plan: cudaMalloc of the workspace failed");
+  }
+  cudaMemset(plan->dwork, 0, bytes);
+  unsigned char* wb = (unsigned char*)plan->dwork;
+  w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
+  w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
+  w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
+  // ---- host copy of the symbolic structure
+  HostSym& hs = plan->sym;
+  hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
+  hs.colptr = colptr; hs.rowidx = rowidx;
+  *out = plan;
+  return WDS_OK;
+}
+
+extern "C" int wds_plan_stats(const WdsPlan* plan, int64_t* o) {
+  if (!plan || !o) return fail(WDS_E_ARG, "wds_plan_stats: bad argument");
+  o[0] = plan->dn.Nj; o[1] = plan->dn.nnzL; o[2] = plan->dn.nlev; o[3] = plan->dn.nfpair;
+  o[4] = (int64_t)plan->smem_fwd; o[5] = plan->dn.npcv; o[6] = plan->nnzA_lower;
+  o[7] = plan->threads;
+  return WDS_OK;
+}
+
+extern "C" int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
+                                 int32_t* rowidx, int32_t* parent, int32_t* level) {
+  if (!plan) return fail(WDS_E_ARG, "wds_plan_symbolic: bad argument");
+  const auto& s = plan->sym;
+  if (perm) std::copy(s.perm.begin(), s.perm.end(), perm);
+  if (colptr) std::copy(s.colptr.begin(), s.colptr.end(), colptr);
+  if (rowidx) std::copy(s.rowidx.begin(), s.rowidx.end(), rowidx);
+  if (parent) std::copy(s.parent.begin(), s.parent.end(), parent);
+  if (level) std::copy(s.level.begin(), s.level.end(), level);
+  return WDS_OK;
+}
+
+extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o,
+                           const double* demand, const double* fixed_head, const double* ke,
+                           const double* r, double* head, double* flow, double* emitter,
+                           int8_t* status, int32_t* iters, double* relerr, int32_t* info,
+                           void* stream) {
+  using namespace wds;
+  if (!plan || !o || batch <= 0) return fail(WDS_E_ARG, "wds_forward: bad argument");
+  if (batch > plan->max_batch) return fail(WDS_E_ARG, "wds_forward: batch exceeds the plan's max_batch");
+  if (!demand || !fixed_head || !ke || !r || !head || !flow || !emitter || !status || !iters ||
+      !relerr || !info)
+    return fail(WDS_E_ARG, "wds_forward: null pointer");
+  if (o->max_iter <= 0 || !(o->accuracy > 0.0) || o->refine < 0)
+    return fail(WDS_E_ARG, "wds_forward: bad options");
+  FwdArgs a{};
+  a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
+  a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
+  a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
+  a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
+  a.relerr = relerr; a.info = info;
+  std::string err;
+  int rc = launch_forward(plan->dn, plan->dw, a, plan->smem_fwd, plan->threads, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  plan->have_state = o->polish_steps >= 0;
+  plan->state_batch = batch;
+  return WDS_OK;
+}
+
+extern "C" int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH, const double* gQ,
+                           const double* gE, double* gd, double* grh, double* gke, double* gr,
+                           void* stream) {
+  using namespace wds;
+  if (!plan || batch <= 0 || !gH || !gQ || !gE || !gd || !grh || !gke || !gr)
+    return fail(WDS_E_ARG, "wds_adjoint: bad argument");
+  if (!plan->have_state || batch != plan->state_batch)
+    return fail(WDS_E_STATE, "wds_adjoint: no implicit forward of this batch size to differentiate");
+  AdjArgs a{batch, gH, gQ, gE, gd, grh, gke, gr};
+  std::string err;
+  int rc = launch_adjoint(plan->dn, plan->dw, a, plan->smem_adj, plan->threads, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  return WDS_OK;
+}
+
+extern "C" int wds_free(WdsPlan* plan) {
+  if (!plan) return WDS_OK;
+  if (plan->dtab) cudaFree(plan->dtab);
+  if (plan->dwork) cudaFree(plan->dwork);
+  delete plan;
+  return WDS_OK;
+}
