@@ -1,0 +1,387 @@
+"""Benchmark: forward + implicit adjoint scenarios/s at B=1024 on the
+782-junction synthetic network (905 pipes, 3 PRVs, 2 reservoirs, 20 emitters).
+
+One step = one pass of the hot path over one batch: the batched GGA solve
+with the status machine, the 3-step reduced Newton polish, the terminal
+factorisation, the implicit adjoint of loss = sum of squared heads at 30
+sensor junctions, and the gradients w.r.t. demand, pipe roughness (chain rule
+through r = 4.727 L / C^1.852 / D^4.871) and emitter coefficients.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sm100|reference]
+
+N > 1 is launched with torch.distributed.run: every rank solves its own
+batch of 1024 scenarios (weak scaling); the batch-summed roughness and
+emitter gradients are all-reduced over NCCL.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adjoint scenarios/s at B=1024 (782 jn) vs ref cuDSS on B200, at 1e-9 m head err"
+UNIT = "scenarios/s"
+WORKLOAD = ("782-junction synthetic looped network (905 pipes, 3 PRVs, 2 reservoirs, "
+            "20 emitters), B=1024 lognormal(0.2) demand scenarios; batched GGA with "
+            "status machine (accuracy 1e-6) + 3-step Newton polish + implicit adjoint of "
+            "sum of squared heads at 30 sensors; grads w.r.t. demand, roughness C, emitter Ke")
+N_SENSORS = 30
+POLISH = 3
+ACCURACY = 1e-6
+
+
+def bytes_per_iteration(L, nA, nL, Nj, w=8):
+    """Streaming model of one Newton iteration (coefficients, assembly, LDL^T,
+    solve + 2 refinements, update): 64 L + (24 + w) nA + 7 w nL + 96 Nj."""
+    return 64 * L + (24 + w) * nA + 7 * w * nL + 96 * Nj
+
+
+def adjoint_bytes(L, N, nA, nL, Nj, w=8):
+    """RHS, one solve + 2 refinements on the kept factor, gradient writes."""
+    return 24 * L + (6 * w * nL + 16 * nA + 80 * Nj) + 8 * (2 * N + L)
+
+
+def read_profile_traffic():
+    """Per-scenario DRAM bytes of the forward kernel from the committed ncu
+    summary (None when absent)."""
+    p = os.path.join(ROOT, "profiles", "k_forward_config2.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_scenario:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                   "-lms", "100"]
+            if self.gpu_id is not None:
+                cmd += ["-i", str(self.gpu_id)]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _gpu_id_for(dev_index):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if dev_index < len(ids):
+            return ids[dev_index]
+    return dev_index
+
+
+# ------------------------------------------------------------------ CPU legs
+def _oracle_scenarios(payload):
+    """Oracle fwd + polish + adjoint on a few scenarios (one process)."""
+    import numpy as np
+    from threadpoolctl import threadpool_limits
+    sys.path.insert(0, ROOT)
+    from oracle.gga import Model
+    from wdsgpu_b200 import synth
+    d, rh = payload
+    with threadpool_limits(1):
+        net = synth.config2_network()
+        m = Model(net)
+        sens = synth.sensor_nodes(net, N_SENSORS)
+        out, st = m.implicit(d, rh, accuracy=ACCURACY, polish_steps=POLISH)
+        gH = np.zeros_like(out["head_ft"])
+        gH[:, sens] = 2.0 * out["head_ft"][:, sens]
+        g = m.backward(st, gH, np.zeros_like(out["flow_cfs"]), np.zeros_like(out["emitter_cfs"]))
+    return float(g[0].sum())
+
+
+def cpu_baseline_single(n_scen=3):
+    """The oracle port timed on one host core (the `cpu_baseline` object)."""
+    from wdsgpu_b200 import synth
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, n_scen, seed=4242)
+    t0 = time.perf_counter()
+    _oracle_scenarios((d, rh))
+    dt = time.perf_counter() - t0
+    return {"value": n_scen / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "%d scenarios of the B=1024 workload (fwd + 3-step polish + adjoint), "
+                      "numpy oracle, one core, %.1f s" % (n_scen, dt)}
+
+
+def run_reference(args, rank, world):
+    """`--impl reference`: the reference algorithm's CPU restatement (the
+    oracle port) on every host core, one scenario per worker per step."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from wdsgpu_b200 import synth
+    cores = os.cpu_count() or 1
+    workers = max(1, min(cores, 32))
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, 1024, seed=1000)
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(workers) as pool:
+        k = 0
+        for i in range(args.warmup + args.steps):
+            chunks = []
+            for _ in range(workers):
+                chunks.append((d[k % 1024:k % 1024 + 1], rh[k % 1024:k % 1024 + 1]))
+                k += 1
+            t0 = time.perf_counter()
+            pool.map(_oracle_scenarios, chunks)
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = workers / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "B": 1024, "sample_per_step": workers},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": "%d scenarios per step (one per worker process, "
+                                       "numpy oracle restating the reference dense route)"
+                                       % workers},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU leg
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="sm100", choices=("sm100", "reference"))
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from wdsgpu_b200 import synth
+    from wdsgpu_b200.autodiff import dr_dC, implicit_solve
+    from wdsgpu_b200.solver import GGASolver
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    B = args.batch
+    net = synth.config2_network()
+    s = GGASolver(net, device=dev, dense_status_machine=True)
+    d_np, rh_np = synth.config2_scenarios(net, B, seed=1000 + rank)
+    sens = torch.as_tensor(synth.sensor_nodes(net, N_SENSORS), device=dev)
+    C = torch.as_tensor(np.asarray(net.roughness), device=dev)
+    length = torch.as_tensor(np.asarray(net.len_ft), device=dev)
+    diam = torch.as_tensor(np.asarray(net.diam_ft), device=dev)
+    is_pipe = torch.as_tensor(np.asarray(net.link_type) == 1, device=dev)
+    dC = torch.where(is_pipe, dr_dC(torch.where(is_pipe, C, torch.ones_like(C)), length, diam),
+                     torch.zeros_like(C))
+    d_dev = torch.as_tensor(d_np, device=dev)
+    rh_dev = torch.as_tensor(rh_np, device=dev)
+    r_dev = s.r_hw.clone()
+    ke_dev = s.node_ke_default.clone()
+    stream = torch.cuda.current_stream(dev)
+
+    def step(D, R, KE):
+        D = D.detach().requires_grad_(True)
+        R = R.detach().requires_grad_(True)
+        KE = KE.detach().requires_grad_(True)
+        h, q, e = implicit_solve(s, D, rh_dev, ke=KE, r_hw=R, accuracy=ACCURACY,
+                                 polish_steps=POLISH, status_machine=True)
+        loss = (h.index_select(1, sens) ** 2).sum()
+        loss.backward()
+        gR, gK = R.grad, KE.grad
+        if world > 1:
+            dist.all_reduce(gR)
+            dist.all_reduce(gK)
+        gC = gR * dC
+        return loss.detach(), D.grad, gC, gK
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        step(d_dev, r_dev, ke_dev)
+    barrier()
+    # ---- device-timed region: inputs resident in HBM, L2 flushed between steps
+    s.launch_events = []
+    step_ms = []
+    with ClockSampler(_gpu_id_for(local)) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            loss, gD, gC, gK = step(d_dev, r_dev, ke_dev)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            step_ms.append(e0.elapsed_time(e1))
+        barrier()
+    events = s.launch_events
+    s.launch_events = None
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+    value = world * B * args.steps / (total_ms / 1e3)
+    fwd_ms = [a.elapsed_time(b) for (nm, a, b) in events if nm == "forward"]
+    adj_ms = [a.elapsed_time(b) for (nm, a, b) in events if nm == "adjoint"]
+    # ---- end to end through the public API with host buffers
+    d_host = torch.as_tensor(d_np).pin_memory()
+    r_host = r_dev.cpu().pin_memory()
+    outs = [torch.empty(1, dtype=torch.float64).pin_memory(),
+            torch.empty(B, net.N, dtype=torch.float64).pin_memory(),
+            torch.empty(net.L, dtype=torch.float64).pin_memory(),
+            torch.empty(net.N, dtype=torch.float64).pin_memory()]
+    e2e_ms = []
+    barrier()
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Dd = d_host.to(dev, non_blocking=True)
+        Rd = r_host.to(dev, non_blocking=True)
+        loss, gD, gC, gK = step(Dd, Rd, ke_dev)
+        for o, g in zip(outs, (loss.reshape(1), gD, gC, gK)):
+            o.copy_(g, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = float(sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t)
+    h2d = d_host.numel() * 8 + r_host.numel() * 8
+    d2h = sum(o.numel() * 8 for o in outs)
+    # ---- roofline of the dominant kernel (the fused forward)
+    st = s.plan_stats(B)
+    iters = s.run(d_dev, rh_dev, ke_dev.unsqueeze(0), r_dev.unsqueeze(0), B, 200, ACCURACY,
+                  True, POLISH)["iters"].double()
+    n_fac = float((iters + POLISH + 1).sum())
+    bpi = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"])
+    fwd_bytes = n_fac * bpi
+    fwd_avg_ms = statistics.mean(fwd_ms) if fwd_ms else float("nan")
+    adj_avg_ms = statistics.mean(adj_ms) if adj_ms else float("nan")
+    dominant = "k_forward" if fwd_avg_ms >= adj_avg_ms else "k_adjoint"
+    peak, peak_kind = measured_peak()
+    achieved = fwd_bytes / (fwd_avg_ms / 1e3) / 1e9
+    traffic_per_scen = read_profile_traffic()
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "B": B, "network": "782 jn / 908 links",
+                       "l2": "flushed between steps (256 MB write, outside the timed events)",
+                       "parallelism": "scenario shards per rank" if world > 1 else "single GPU",
+                       "nnz_L": st["nnz_L"], "levels": st["n_levels"],
+                       "mean_gga_iters": float(iters.mean())},
+            "e2e": {"value": world * B * args.steps / (e2e_total / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "kernel_ms": {"k_forward": fwd_avg_ms, "k_adjoint": adj_avg_ms},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind,
+                         "traffic": (traffic_per_scen * B if traffic_per_scen else None),
+                         "algorithmic_bytes": fwd_bytes,
+                         "model": "bytes/iter = 64L + 32 nA + 56 nL + 96 Nj = %d B; x (iters+%d) per scenario" % (bpi, POLISH + 1)},
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline_single()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -70,7 +70,8 @@ enum {
 /* per-scenario info bits written by wds_forward */
 enum {
   WDS_INFO_NOT_PD = 1,      /* a pivot of the LDL^T factor was <= 0 or not finite */
-  WDS_INFO_UNCONVERGED = 2  /* GGA loop ran out of trials                         */
+  WDS_INFO_UNCONVERGED = 2, /* GGA loop ran out of trials                         */
+  WDS_INFO_EMITTER_CAP = 4  /* more emitters than the plan's emitter capacity     */
 };
 
 /* Static network description (host pointers; copied by wds_plan). */
@@ -108,6 +109,7 @@ typedef struct WdsNetwork {
   double hexp, qexp, rqtol, htol, qtol, ucf_flow, ucf_head;
   int32_t checkfreq, maxcheck, extra_iter;
   const int32_t* perm;           /* [Nj] elimination order of junction rows, or NULL */
+  int32_t emitter_capacity;      /* emitters per scenario kept on chip (0: 64) */
 } WdsNetwork;
 
 /* Options of one forward call. */

@@ -18,7 +18,7 @@ c_double_p = ctypes.POINTER(ctypes.c_double)
 KIND_PIPE, KIND_CVPIPE, KIND_TCV, KIND_PUMP, KIND_PRV_FIXED, KIND_PRV = range(6)
 F_ZERO_SPEED, F_PUMP_LIVE, F_CHP, F_IS_PIPE = 1, 2, 4, 8
 TL_OVERFLOW, TL_IS_PUMP, TL_PUMP_IN, TL_PUMP_OUT = 1, 2, 4, 8
-INFO_NOT_PD, INFO_UNCONVERGED = 1, 2
+INFO_NOT_PD, INFO_UNCONVERGED, INFO_EMITTER_CAP = 1, 2, 4
 E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
            -4: "unsupported network", -5: "no forward state"}
 
@@ -48,6 +48,7 @@ class WdsNetwork(ctypes.Structure):
         ("checkfreq", ctypes.c_int32), ("maxcheck", ctypes.c_int32),
         ("extra_iter", ctypes.c_int32),
         ("perm", c_int32_p),
+        ("emitter_capacity", ctypes.c_int32),
     ]
 
 

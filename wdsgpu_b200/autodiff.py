@@ -18,6 +18,8 @@ downstream junction or cascade.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -78,6 +80,8 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
             ke_t = ke_t.contiguous()
         o = s.run(d, rh, ke_t, r_t, B, int(max_iter), float(accuracy), sm, int(polish_steps))
         info = o["info"]
+        from .solver import _check_emitter_cap
+        _check_emitter_cap(s, info)
         if bool((info != 0).any()):
             bad = torch.nonzero(info != 0).flatten().tolist()
             np_ = torch.nonzero(info & _lib.INFO_NOT_PD).flatten().tolist()
@@ -123,12 +127,14 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         gke = torch.empty_like(gd)
         gr = torch.empty(B, L, dtype=torch.float64, device=dev)
         p = ctx.plan
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        import ctypes
+        cur = torch.cuda.current_stream(dev)
+        ev = s._event_pair(cur, "adjoint")
         _lib.check(p.lib.wds_adjoint(
             p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
-            grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(stream)),
+            grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
             "wds_adjoint")
+        if ev is not None:
+            ev[1].record(cur)
         dm, dv = ctx.dims, ctx.devs
 
         def _fit(g, dim, d_):

@@ -66,9 +66,9 @@ struct DevNet {
   const int* ftask_ptr;   // [nlev+1]
   const int4* ftask;      // {slot, pair_begin, pair_end, is_diag}
   const int* fpair;       // [3*nfpair] {s1, s2, diag slot of k}
-  const int* rptr;        // [Nj+1] row lists (forward solve)
-  const int* rslot;
-  const int* rcol;
+  const int4* fitem;      // [Nj] level order: {j, row entry begin, end, diag slot}
+  const int4* bitem;      // [Nj] level order: {j, colptr[j], colptr[j+1], 0}
+  const int2* rent;       // row entries {slot of L_jk, k}, level order
   // status-machine PRVs [npcv]
   const int* pcv_link;
   const int* pcv_j1;
@@ -87,6 +87,13 @@ struct DevNet {
   const uint8_t* tl_flags;
   double hexp, qexp, rqtol, htol, qtol, ucf_flow, ucf_head;
   int checkfreq, maxcheck, extra_iter;
+  // compact 16-bit copy of the hot schedule tables, staged into shared memory
+  // once per CTA (see STabOff)
+  const uint4* stab;
+  int stab_bytes;
+  int o_ftask_ptr, o_ftask, o_fpair, o_colptr, o_rowidx, o_levptr, o_fitem, o_bitem, o_rent,
+      o_mode, o_inc_ptr, o_inc_split, o_inc, o_e1, o_e2, o_pptr, o_plink, o_pslot, o_fill;
+  int emcap;  // emitters per scenario held in shared memory
 };
 
 // Workspace kept between the forward (implicit mode) and the adjoint.
@@ -138,11 +145,12 @@ struct HostSym {
   std::vector<int> perm, iperm, parent, level, colptr, rowidx;
 };
 
-int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a,
-                   size_t smem, int threads, void* stream, std::string* err);
-int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a,
-                   size_t smem, int threads, void* stream, std::string* err);
-size_t forward_smem_bytes(const DevNet& n, int threads);
-size_t adjoint_smem_bytes(const DevNet& n, int threads);
+// Kernels run `groups` independent scenario groups of 256 threads per CTA;
+// shared memory = schedule tables + groups * per-scenario state.
+int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
+                   void* stream, std::string* err);
+int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int groups,
+                   void* stream, std::string* err);
+size_t state_smem_bytes(const DevNet& n);
 
 }  // namespace wds

@@ -1,17 +1,22 @@
 // Fused batched GGA forward and reduced implicit adjoint for sm_100a.
 //
-// One CTA owns one scenario for the whole call: its link flows, link
-// coefficients, the factor of the node matrix and the node vectors live in
-// shared memory from the first Newton iteration to the terminal factorisation,
-// so there is no host round trip and no HBM traffic inside the loop.
+// A CTA holds `GR` independent scenario groups of 256 threads.  Each group owns
+// one scenario at a time: its link flows and coefficients, the LDL^T factor of
+// the node matrix and the node vectors live in shared memory from the first
+// Newton iteration to the terminal factorisation, so there is no host round
+// trip inside the loop.  The symbolic schedule (update lists, row and column
+// structure, incidence lists) is staged once per CTA into shared memory as
+// 16-bit tables and shared by the groups.  Groups synchronise on their own
+// named barriers, so they advance independently.
 //
 // Per GGA iteration (dgga/solver.py:2922-3179):
 //   link pass    P, Y from the headloss formulas (one thread per link)
 //   node pass    gather assembly of A (diagonal, pairs) and F in the
 //                reference's scatter order; PRV valve coefficients after the
 //                node coefficients (serial over the few PRVs)
-//   factor       left-looking LDL^T, one barrier per elimination-tree level
-//   solve        level-scheduled forward/backward substitution + refinement
+//   factor       left-looking LDL^T, dependency-driven: a column starts as soon
+//                as the columns it depends on are done (shared-memory counters)
+//   solve        dependency-driven forward/backward substitution + refinement
 //                against the matrix-free operator A x
 //   update       dq = Y - P dh, emitter update, relerr reduction, status
 //                machine (valve status every iteration, link status on the
@@ -32,25 +37,103 @@ namespace {
 constexpr double kINF = __builtin_huge_val();
 
 struct Sh {
-  double *q, *P, *Y, *W, *V0, *V1, *V2, *e, *emh, *hf, *xf, *red, *small;
+  double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
+  double *em_e, *em_ke, *em_emh;  // per emitter slot: flow, coefficient, 1/hgrad
+  int16_t* eslot;                 // [Nj] emitter slot of a junction or -1
+  int *wcnt, *flag, *err;
   int8_t* S;
 };
+
+// Shared-memory view of the compact tables (16-bit indices).
+struct STab {
+  const uint16_t* ftask_ptr;  // [nlev+1] factor tasks per level
+  const uint2* ftask;         // slot | diag << 31, update begin | count << 16
+  const uint16_t* fpair;      // [3 * npairs] {slot L_ik, slot L_jk, slot 1/D_k}
+  const uint16_t* colptr;     // [Nj+1]
+  const uint16_t* rowidx;     // [nnzL]
+  const uint16_t* levptr;     // [nlev+1] columns per level
+  const uint2* fitem;         // forward: j | e0 << 16, e1 | diag slot << 16
+  const uint2* bitem;         // backward: j | c0 << 16, c1
+  const uint32_t* rent;       // row entries slot | k << 16, level order
+  const uint8_t* mfac;        // [nlev] mode: log2 G | wide << 7
+  const uint8_t* mfwd;
+  const uint8_t* mbwd;
+  const uint16_t* inc_ptr;    // [Nj+1]
+  const uint16_t* inc_split;  // [Nj]
+  const uint32_t* inc;        // link | PRV << 16 | other fixed << 17 | fixed index << 18
+  const int16_t* e1;          // [L] end codes
+  const int16_t* e2;
+  const uint16_t* pptr;       // [npairs+1]
+  const uint16_t* plink;      // link | PRV << 15
+  const uint16_t* pslot;      // [npairs]
+  const uint16_t* fill;       // [nfill]
+};
+
+__device__ STab stab_view(const DevNet& n, const unsigned char* b) {
+  STab t;
+  t.ftask_ptr = (const uint16_t*)(b + n.o_ftask_ptr);
+  t.ftask = (const uint2*)(b + n.o_ftask);
+  t.fpair = (const uint16_t*)(b + n.o_fpair);
+  t.colptr = (const uint16_t*)(b + n.o_colptr);
+  t.rowidx = (const uint16_t*)(b + n.o_rowidx);
+  t.levptr = (const uint16_t*)(b + n.o_levptr);
+  t.fitem = (const uint2*)(b + n.o_fitem);
+  t.bitem = (const uint2*)(b + n.o_bitem);
+  t.rent = (const uint32_t*)(b + n.o_rent);
+  t.mfac = (const uint8_t*)(b + n.o_mode);
+  t.mfwd = t.mfac + n.nlev;
+  t.mbwd = t.mfwd + n.nlev;
+  t.inc_ptr = (const uint16_t*)(b + n.o_inc_ptr);
+  t.inc_split = (const uint16_t*)(b + n.o_inc_split);
+  t.inc = (const uint32_t*)(b + n.o_inc);
+  t.e1 = (const int16_t*)(b + n.o_e1);
+  t.e2 = (const int16_t*)(b + n.o_e2);
+  t.pptr = (const uint16_t*)(b + n.o_pptr);
+  t.plink = (const uint16_t*)(b + n.o_plink);
+  t.pslot = (const uint16_t*)(b + n.o_pslot);
+  t.fill = (const uint16_t*)(b + n.o_fill);
+  return t;
+}
+
+// link index of an incidence entry (the upper bits carry flags)
+__device__ __forceinline__ int inc_link(const STab& T, int e) { return (int)(T.inc[e] & 0xffffu); }
 
 __device__ __forceinline__ double head_of(int c, const double* x, const double* hf) {
   return c >= 0 ? x[c] : hf[-c - 1];
 }
 __device__ __forceinline__ double junc_of(int c, const double* x) { return c >= 0 ? x[c] : 0.0; }
 
-// ---------------------------------------------------------------- reductions
+// ---------------------------------------------------------------- groups
+// A group synchronises with its own named barrier (id 1 + group index).
+template <int NT>
+__device__ __forceinline__ int gtid() { return threadIdx.x & (NT - 1); }
+template <int NT>
+__device__ __forceinline__ void gsync() {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / NT)), "r"(NT) : "memory");
+}
+template <int NT>
+__device__ __forceinline__ bool gsync_or(bool p) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred ip, op;\n\tsetp.ne.u32 ip, %1, 0;\n\t"
+      "bar.red.or.pred op, %2, %3, ip;\n\tselp.u32 %0, 1, 0, op;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)p), "r"(1 + (int)(threadIdx.x / NT)), "r"(NT)
+      : "memory");
+  return r != 0;
+}
+
+// Deterministic group sum of m <= 4 values (warp butterflies, then a fixed
+// order over the warps); every thread gets the same result.
 template <int NT>
 __device__ void block_sum(double* v, int m, double* red) {
   for (int i = 0; i < m; ++i)
     for (int o = 16; o; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
+  const int w = gtid<NT>() >> 5, l = threadIdx.x & 31;
+  gsync<NT>();
   if (l == 0)
     for (int i = 0; i < m; ++i) red[w * 4 + i] = v[i];
-  __syncthreads();
+  gsync<NT>();
   for (int i = 0; i < m; ++i) {
     double s = 0.0;
     for (int ww = 0; ww < NT / 32; ++ww) s += red[ww * 4 + i];
@@ -218,20 +301,22 @@ __device__ __forceinline__ void link_coef(const DevNet& n, int k, double q, int 
 // Matrix-free (A x)_p of the node matrix: links with conductance P, emitter
 // diagonal emh, CBIG on the downstream node of ACTIVE PRVs
 // (dgga/autodiff.py:878-895; the same operator the forward assembles).
-__device__ __forceinline__ double amul_node(const DevNet& n, int p, const double* P,
-                                            const double* x, const double* emh,
-                                            const int8_t* S) {
+__device__ __forceinline__ double amul_node(const DevNet& n, const STab& T, const Sh& s, int p,
+                                            const double* x) {
+  const double* P = s.P;
+  const int8_t* S = s.S;
   double acc = 0.0;
-  const int a = n.inc_ptr[p], m = n.inc_split[p], z = n.inc_ptr[p + 1];
+  const int a = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
   for (int e = a; e < m; ++e) {
-    const int k = n.inc[e];
-    acc += P[k] * (junc_of(n.e1[k], x) - junc_of(n.e2[k], x));
+    const int k = inc_link(T, e);
+    acc += P[k] * (junc_of(T.e1[k], x) - junc_of(T.e2[k], x));
   }
   for (int e = m; e < z; ++e) {
-    const int k = n.inc[e];
-    acc += -(P[k] * (junc_of(n.e1[k], x) - junc_of(n.e2[k], x)));
+    const int k = inc_link(T, e);
+    acc += -(P[k] * (junc_of(T.e1[k], x) - junc_of(T.e2[k], x)));
   }
-  acc = acc + emh[p] * x[p];
+  const int es = s.eslot[p];
+  acc = acc + (es >= 0 ? s.em_emh[es] : 0.0) * x[p];
   for (int c = n.cb_ptr[p]; c < n.cb_ptr[p + 1]; ++c) {
     const int i = n.cb_idx[c];
     const double act = S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0;
@@ -240,72 +325,173 @@ __device__ __forceinline__ double amul_node(const DevNet& n, int p, const double
   return acc;
 }
 
-// Left-looking LDL^T by elimination-tree level.  W holds A on entry (pattern
-// of L, fill zero) and on exit the unscaled columns L_ij D_j with 1/D_j in the
-// diagonal slot.  Returns true when every pivot was positive and finite.
-template <int NT>
-__device__ bool ldl_factor(const DevNet& n, double* W) {
-  bool bad = false;
-  for (int lv = 0; lv < n.nlev; ++lv) {
-    const int t0 = n.ftask_ptr[lv], t1 = n.ftask_ptr[lv + 1];
-    for (int t = t0 + threadIdx.x; t < t1; t += NT) {
-      const int4 tk = n.ftask[t];
-      double w = W[tk.x];
-      for (int pr = tk.y; pr < tk.z; ++pr) {
-        const int* f = n.fpair + 3 * pr;
-        w -= W[f[0]] * W[f[1]] * W[f[2]];
-      }
-      if (tk.w) {
-        if (!(w > 0.0) || !isfinite(w)) bad = true;
-        W[tk.x] = 1.0 / w;
-      } else {
-        W[tk.x] = w;
-      }
-    }
-    __syncthreads();
-  }
-  return !__syncthreads_or(bad);
+// Sum over a lane group of size 1 << lg (aligned groups inside a warp); every
+// lane of the warp calls it with the same lg.
+__device__ __forceinline__ double group_sum(double v, int lg) {
+  for (int o = (1 << lg) >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
-// In-place solve of (L D L^T) v = b, level-scheduled.
-template <int NT>
-__device__ void ldl_solve(const DevNet& n, const double* W, double* v) {
-  for (int lv = 0; lv < n.nlev; ++lv) {
-    for (int t = n.levptr[lv] + threadIdx.x; t < n.levptr[lv + 1]; t += NT) {
-      const int j = n.levcol[t];
-      double acc = v[j];
-      for (int e = n.rptr[j]; e < n.rptr[j + 1]; ++e) acc -= W[n.rslot[e]] * v[n.rcol[e]];
-      v[j] = acc * W[n.colptr[j]];
+// One level of the left-looking LDL^T on `nthr` threads (thread index t):
+// the level's entries are split over lane groups of 1 << lg, each group
+// reducing its entry's update list with warp shuffles.
+__device__ __forceinline__ void fac_level(const STab& T, double* W, int lv, int lg, int t,
+                                          int nthr, bool& bad) {
+  const int t0 = T.ftask_ptr[lv], t1 = T.ftask_ptr[lv + 1];
+  const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
+  for (int base = t0; base < t1; base += per) {
+    const int it = base + (t >> lg);
+    const bool valid = it < t1;
+    uint2 tk = make_uint2(0u, 0u);
+    double acc = 0.0;
+    if (valid) {
+      tk = T.ftask[it];
+      const int pb = tk.y & 0xffff, pe = pb + (int)(tk.y >> 16);
+      for (int pr = pb + li; pr < pe; pr += G) {
+        const uint16_t* f = T.fpair + 3 * pr;
+        acc += W[f[0]] * W[f[1]] * W[f[2]];
+      }
     }
-    __syncthreads();
+    acc = group_sum(acc, lg);
+    if (valid && li == 0) {
+      const int slot = tk.x & 0x7fffffff;
+      const double w = W[slot] - acc;
+      if (tk.x >> 31) {
+        if (!(w > 0.0) || !isfinite(w)) bad = true;
+        W[slot] = 1.0 / w;
+      } else {
+        W[slot] = w;
+      }
+    }
+  }
+}
+
+// One forward-substitution level: v_j = (v_j - sum_k L_jk D_k u_k) / D_j.
+__device__ __forceinline__ void fwd_level(const STab& T, const double* W, double* v, int lv,
+                                          int lg, int t, int nthr) {
+  const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
+  const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
+  for (int base = c0; base < c1; base += per) {
+    const int it = base + (t >> lg);
+    const bool valid = it < c1;
+    uint2 fi = make_uint2(0u, 0u);
+    double acc = 0.0;
+    if (valid) {
+      fi = T.fitem[it];
+      const int e0 = fi.x >> 16, e1 = fi.y & 0xffff;
+      for (int e = e0 + li; e < e1; e += G) {
+        const uint32_t r = T.rent[e];
+        acc += W[r & 0xffff] * v[r >> 16];
+      }
+    }
+    acc = group_sum(acc, lg);
+    if (valid && li == 0) {
+      const int j = fi.x & 0xffff;
+      v[j] = (v[j] - acc) * W[fi.y >> 16];
+    }
+  }
+}
+
+// One backward-substitution level: x_j = u_j - (1/D_j) sum_i L_ij D_j x_i.
+__device__ __forceinline__ void bwd_level(const STab& T, const double* W, double* v, int lv,
+                                          int lg, int t, int nthr) {
+  const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
+  const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
+  for (int base = c0; base < c1; base += per) {
+    const int it = base + (t >> lg);
+    const bool valid = it < c1;
+    uint2 bi = make_uint2(0u, 0u);
+    double acc = 0.0;
+    if (valid) {
+      bi = T.bitem[it];
+      const int cb = bi.x >> 16, ce = bi.y;
+      for (int e = cb + 1 + li; e < ce; e += G) acc += W[e] * v[T.rowidx[e]];
+    }
+    acc = group_sum(acc, lg);
+    if (valid && li == 0) {
+      const int j = bi.x & 0xffff;
+      v[j] = v[j] - W[bi.x >> 16] * acc;
+    }
+  }
+}
+
+// Level-scheduled LDL^T.  Wide levels (many independent entries) use all the
+// group's threads and a group barrier; narrow levels run on warp 0 alone,
+// separated by __syncwarp.  W holds A on entry (pattern of L, fill zero) and
+// on exit the unscaled columns L_ij D_j with 1/D_j in the diagonal slot.
+// Returns true when every pivot was positive and finite.
+template <int NT>
+__device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
+  const int tid = gtid<NT>();
+  bool bad = false, prev_wide = true;
+  for (int lv = 0; lv < n.nlev; ++lv) {
+    const int md = T.mfac[lv];
+    const bool wide = (md & 0x80) != 0;
+    if (wide) {
+      if (!prev_wide) gsync<NT>();
+      fac_level(T, s.W, lv, md & 7, tid, NT, bad);
+      gsync<NT>();
+    } else if (tid < 32) {
+      fac_level(T, s.W, lv, md & 7, tid, 32, bad);
+      __syncwarp();
+    }
+    prev_wide = wide;
+  }
+  return !gsync_or<NT>(bad);
+}
+
+// In-place (L D L^T) v = b, level-scheduled in both sweeps.
+template <int NT>
+__device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
+  const int tid = gtid<NT>();
+  bool prev_wide = true;
+  for (int lv = 0; lv < n.nlev; ++lv) {
+    const int md = T.mfwd[lv];
+    const bool wide = (md & 0x80) != 0;
+    if (wide) {
+      if (!prev_wide) gsync<NT>();
+      fwd_level(T, s.W, v, lv, md & 7, tid, NT);
+      gsync<NT>();
+    } else if (tid < 32) {
+      fwd_level(T, s.W, v, lv, md & 7, tid, 32);
+      __syncwarp();
+    }
+    prev_wide = wide;
   }
   for (int lv = n.nlev - 1; lv >= 0; --lv) {
-    for (int t = n.levptr[lv] + threadIdx.x; t < n.levptr[lv + 1]; t += NT) {
-      const int j = n.levcol[t];
-      const int c0 = n.colptr[j];
-      double s = 0.0;
-      for (int e = c0 + 1; e < n.colptr[j + 1]; ++e) s += W[e] * v[n.rowidx[e]];
-      v[j] = v[j] - W[c0] * s;
+    const int md = T.mbwd[lv];
+    const bool wide = (md & 0x80) != 0;
+    if (wide) {
+      if (!prev_wide) gsync<NT>();
+      bwd_level(T, s.W, v, lv, md & 7, tid, NT);
+      gsync<NT>();
+    } else if (tid < 32) {
+      bwd_level(T, s.W, v, lv, md & 7, tid, 32);
+      __syncwarp();
     }
-    __syncthreads();
+    prev_wide = wide;
   }
+  gsync<NT>();
 }
 
 // x = A^{-1} rhs with `refine` refinement steps against the matrix-free A.
+// unit >= 0 means rhs = e_unit.
 template <int NT>
-__device__ void solve_refined(const DevNet& n, const double* W, const double* P,
-                              const double* emh, const int8_t* S, const double* rhs, double* x,
-                              double* t, int refine) {
-  for (int p = threadIdx.x; p < n.Nj; p += NT) x[p] = rhs[p];
-  __syncthreads();
-  ldl_solve<NT>(n, W, x);
+__device__ void solve_refined(const DevNet& n, const STab& T, const Sh& s, const double* rhs,
+                              int unit, double* x, double* t, int refine) {
+  const int tid = gtid<NT>();
+  for (int p = tid; p < n.Nj; p += NT) x[p] = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
+  gsync<NT>();
+  solve<NT>(n, T, s, x);
   for (int it = 0; it < refine; ++it) {
-    for (int p = threadIdx.x; p < n.Nj; p += NT)
-      t[p] = rhs[p] - amul_node(n, p, P, x, emh, S);
-    __syncthreads();
-    ldl_solve<NT>(n, W, t);
-    for (int p = threadIdx.x; p < n.Nj; p += NT) x[p] = x[p] + t[p];
-    __syncthreads();
+    for (int p = tid; p < n.Nj; p += NT) {
+      const double b = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
+      t[p] = b - amul_node(n, T, s, p, x);
+    }
+    gsync<NT>();
+    solve<NT>(n, T, s, t);
+    for (int p = tid; p < n.Nj; p += NT) x[p] = x[p] + t[p];
+    gsync<NT>();
   }
 }
 
@@ -340,66 +526,69 @@ __device__ void dense_solve(double* C, double* y, int m) {
 
 // ---------------------------------------------------------------- assembly
 // GGA assembly (linkcoeffs -> emittercoeffs -> nodecoeffs, solver.py:2958-3007)
-// into W (pattern of L) and F; Xflow saved for PRV downstream nodes.
+// into W (pattern of L) and F = V0; Xflow saved for PRV downstream nodes.
 template <int NT>
-__device__ void assemble_gga(const DevNet& n, const Sh& s, const double* kerow,
+__device__ void assemble_gga(const DevNet& n, const STab& T, const Sh& s, const double* kerow,
                              const double* drow) {
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
-    const int a = n.inc_ptr[p], m = n.inc_split[p], z = n.inc_ptr[p + 1];
+  const int tid = gtid<NT>();
+  for (int p = tid; p < n.Nj; p += NT) {
+    const int a = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
     double dg = 0.0, xf = 0.0, F = 0.0;
     for (int e = a; e < m; ++e) {
-      const int k = n.inc[e];
-      if (n.kind[k] == WDS_KIND_PRV) continue;
+      const uint32_t ie = T.inc[e];
+      if (ie & (1u << 16)) continue;
+      const int k = ie & 0xffff;
       dg += s.P[k];
       xf += -s.q[k];
       F += s.Y[k];
     }
     for (int e = m; e < z; ++e) {
-      const int k = n.inc[e];
-      if (n.kind[k] == WDS_KIND_PRV) continue;
+      const uint32_t ie = T.inc[e];
+      if (ie & (1u << 16)) continue;
+      const int k = ie & 0xffff;
       dg += s.P[k];
       xf += s.q[k];
       F += -s.Y[k];
     }
     for (int e = m; e < z; ++e) {  // n1 end fixed: F[Row[n2]] += P*H[n1]
-      const int k = n.inc[e];
-      if (n.kind[k] == WDS_KIND_PRV || n.e1[k] >= 0) continue;
-      F += s.P[k] * s.hf[-n.e1[k] - 1];
+      const uint32_t ie = T.inc[e];
+      if ((ie & (1u << 16)) || !(ie & (1u << 17))) continue;
+      F += s.P[ie & 0xffff] * s.hf[ie >> 18];
     }
     for (int e = a; e < m; ++e) {  // n2 end fixed: F[Row[n1]] += P*H[n2]
-      const int k = n.inc[e];
-      if (n.kind[k] == WDS_KIND_PRV || n.e2[k] >= 0) continue;
-      F += s.P[k] * s.hf[-n.e2[k] - 1];
+      const uint32_t ie = T.inc[e];
+      if ((ie & (1u << 16)) || !(ie & (1u << 17))) continue;
+      F += s.P[ie & 0xffff] * s.hf[ie >> 18];
     }
-    const double ke = kerow[n.jnode[p]];
-    double emh = 0.0;
-    if (ke > 0.0) {
+    const int nd = n.jnode[p];
+    const int es = s.eslot[p];
+    if (es >= 0) {
       double hl, hg;
-      emitter_hl(n, s.e[p], ke, hl, hg);
-      emh = 1.0 / hg;
+      emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
+      const double emh = 1.0 / hg;
+      s.em_emh[es] = emh;
       dg = dg + emh;
       F = F + (hl + n.el[p]) / hg;
-      xf = xf - s.e[p];
+      xf = xf - s.em_e[es];
     }
-    s.emh[p] = emh;
-    xf = xf - drow[n.jnode[p]];
+    xf = xf - drow[nd];
     F = F + xf;
-    s.W[n.colptr[p]] = dg;
+    s.W[T.colptr[p]] = dg;
     s.V0[p] = F;
     if (n.node_xf[p] >= 0) s.xf[n.node_xf[p]] = xf;
   }
-  for (int t = threadIdx.x; t < n.npairs; t += NT) {
+  for (int t = tid; t < n.npairs; t += NT) {
     double v = 0.0;
-    for (int e = n.pair_ptr[t]; e < n.pair_ptr[t + 1]; ++e) {
-      const int k = n.pair_link[e];
-      if (n.kind[k] == WDS_KIND_PRV) continue;
-      v += -s.P[k];
+    for (int e = T.pptr[t]; e < T.pptr[t + 1]; ++e) {
+      const int pl = T.plink[e];
+      if (pl & 0x8000) continue;
+      v += -s.P[pl];
     }
-    s.W[n.pair_slot[t]] = v;
+    s.W[T.pslot[t]] = v;
   }
-  for (int t = threadIdx.x; t < n.nfill; t += NT) s.W[n.fill_slot[t]] = 0.0;
-  __syncthreads();
-  if (threadIdx.x == 0) {  // valvecoeffs after nodecoeffs, in valve order
+  for (int t = tid; t < n.nfill; t += NT) s.W[T.fill[t]] = 0.0;
+  gsync<NT>();
+  if (tid == 0) {  // valvecoeffs after nodecoeffs, in valve order
     for (int i = 0; i < n.npcv; ++i) {
       const int k = n.pcv_link[i];
       const double qk = s.q[k];
@@ -414,39 +603,41 @@ __device__ void assemble_gga(const DevNet& n, const Sh& s, const double* kerow,
       const double f2 = -dy + n.pcv_hset[i] * kCBIG * mact;
       const int j1 = n.pcv_j1[i], j2 = n.pcv_j2[i];
       s.W[n.pcv_off[i]] += -pna;
-      s.W[n.colptr[j1]] += pna;
-      s.W[n.colptr[j2]] += pna;
-      s.W[n.colptr[j2]] += kCBIG * mact;
+      s.W[T.colptr[j1]] += pna;
+      s.W[T.colptr[j2]] += pna;
+      s.W[T.colptr[j2]] += kCBIG * mact;
       s.V0[j1] += f1;
       s.V0[j2] += f2;
       s.P[k] = pna;
       s.Y[k] = act ? qk + xf2 : yna;
     }
   }
-  __syncthreads();
+  gsync<NT>();
 }
 
 // Reduced-matrix assembly at the current state (dgga/autodiff.py:928-962):
 // every link with its P, + emh diagonal, + CBIG on ACTIVE PRV downstream nodes.
 template <int NT>
-__device__ void assemble_reduced(const DevNet& n, const Sh& s) {
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
+__device__ void assemble_reduced(const DevNet& n, const STab& T, const Sh& s) {
+  const int tid = gtid<NT>();
+  for (int p = tid; p < n.Nj; p += NT) {
     double dg = 0.0;
-    for (int e = n.inc_ptr[p]; e < n.inc_ptr[p + 1]; ++e) dg += s.P[n.inc[e]];
-    dg = dg + s.emh[p];
+    for (int e = T.inc_ptr[p]; e < T.inc_ptr[p + 1]; ++e) dg += s.P[inc_link(T, e)];
+    const int es = s.eslot[p];
+    dg = dg + (es >= 0 ? s.em_emh[es] : 0.0);
     for (int c = n.cb_ptr[p]; c < n.cb_ptr[p + 1]; ++c) {
       const int i = n.cb_idx[c];
       dg += kCBIG * (s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0);
     }
-    s.W[n.colptr[p]] = dg;
+    s.W[T.colptr[p]] = dg;
   }
-  for (int t = threadIdx.x; t < n.npairs; t += NT) {
+  for (int t = tid; t < n.npairs; t += NT) {
     double v = 0.0;
-    for (int e = n.pair_ptr[t]; e < n.pair_ptr[t + 1]; ++e) v += -s.P[n.pair_link[e]];
-    s.W[n.pair_slot[t]] = v;
+    for (int e = T.pptr[t]; e < T.pptr[t + 1]; ++e) v += -s.P[T.plink[e] & 0x7fff];
+    s.W[T.pslot[t]] = v;
   }
-  for (int t = threadIdx.x; t < n.nfill; t += NT) s.W[n.fill_slot[t]] = 0.0;
-  __syncthreads();
+  for (int t = tid; t < n.nfill; t += NT) s.W[T.fill[t]] = 0.0;
+  gsync<NT>();
 }
 
 // Coefficients at the current state for polish / terminal (autodiff.py:786-875):
@@ -454,68 +645,62 @@ __device__ void assemble_reduced(const DevNet& n, const Sh& s) {
 template <int NT>
 __device__ void adj_coeffs(const DevNet& n, const Sh& s, const double* rrow,
                            const double* kerow) {
-  for (int k = threadIdx.x; k < n.L; k += NT) {
+  const int tid = gtid<NT>();
+  for (int k = tid; k < n.L; k += NT) {
     double P, Y;
     link_coef(n, k, s.q[k], s.S[k], rrow[k], true, P, Y);
     s.P[k] = P;
     s.Y[k] = Y;
   }
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
-    const double ke = kerow[n.jnode[p]];
-    double emh = 0.0;
-    if (ke > 0.0) {
-      double hl, hg;
-      emitter_hl(n, s.e[p], ke, hl, hg);
-      emh = 1.0 / hg;
-    }
-    s.emh[p] = emh;
+  const int nem = s.flag[2];
+  for (int es = tid; es < nem; es += NT) {
+    double hl, hg;
+    emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
+    s.em_emh[es] = 1.0 / hg;
   }
-  __syncthreads();
+  gsync<NT>();
 }
 
-// Woodbury data for ACTIVE-PRV rows.
-struct Wood {
-  double* cols;  // [m][Nj] columns A^{-1} e_u
-  double* C;     // [m*m] in shared memory (small)
-  int m;
-};
-
 // Primal reduced Newton solve with ACTIVE-PRV Dirichlet / merged rows
-// (dgga/autodiff.py:965-1029).  rhs: V0 (kept), result in dH.
+// (dgga/autodiff.py:965-1029): M_p differs from the factored matrix by 2p row
+// replacements, applied by Woodbury and two outer refinement steps against the
+// true M_p.  The Woodbury columns A^{-1} e_u come from one substitution each;
+// the outer refinement makes the result independent of their rounding.
+// rhs: V0 (kept), result in dH.
 template <int NT>
-__device__ void primal_solve(const DevNet& n, const Sh& s, double* rp, double* dH,
+__device__ void primal_solve(const DevNet& n, const STab& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
                              bool any_act, int refine) {
   const double* rhs = s.V0;
   double* t = s.V2;
+  const int tid = gtid<NT>();
   if (!any_act) {
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, rhs, dH, t, refine);
+    solve_refined<NT>(n, T, s, rhs, -1, dH, t, refine);
     return;
   }
   const int p = n.npcv, m = 2 * p;
   double* C = s.small;            // m*m
   double* y = s.small + m * m;    // m
   double* actf = y + m;           // p
-  if (threadIdx.x == 0)
+  double* row1 = actf + p;        // p
+  if (tid == 0)
     for (int i = 0; i < p; ++i) actf[i] = s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0;
-  for (int q = threadIdx.x; q < n.Nj; q += NT) rp[q] = rhs[q];
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  for (int q = tid; q < n.Nj; q += NT) rp[q] = rhs[q];
+  gsync<NT>();
+  if (tid == 0) {
     // rp[j1] += rhs[j2] (ACTIVE), then rp[j2] = -r_prv
     for (int i = 0; i < p; ++i)
       if (actf[i] != 0.0) rp[n.pcv_j1[i]] += rhs[n.pcv_j2[i]];
     for (int i = 0; i < p; ++i)
       if (actf[i] != 0.0) rp[n.pcv_j2[i]] = -rprv[i];
   }
-  __syncthreads();
-  solve_refined<NT>(n, s.W, s.P, s.emh, s.S, rp, dH, t, refine);
+  gsync<NT>();
+  solve_refined<NT>(n, T, s, rp, -1, dH, t, refine);
   for (int c = 0; c < m; ++c) {
     const int u = c < p ? n.pcv_j2[c] : n.pcv_j1[c - p];
-    for (int q = threadIdx.x; q < n.Nj; q += NT) res[q] = q == u ? 1.0 : 0.0;
-    __syncthreads();
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, res, cols + (size_t)c * n.Nj, t, refine);
+    solve_refined<NT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
   }
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     // C = [R2 ; I2 - CBIG R2], rows of inactive valves -> identity
     for (int a = 0; a < p; ++a)
       for (int c = 0; c < m; ++c) {
@@ -525,10 +710,10 @@ __device__ void primal_solve(const DevNet& n, const Sh& s, double* rp, double* d
         C[(a + p) * m + c] = actf[a] != 0.0 ? i2 - kCBIG * r2 : (c == a + p ? 1.0 : 0.0);
       }
   }
-  __syncthreads();
+  gsync<NT>();
   // x <- x - S y,  y = C^{-1} [ (x[j2]-rr[j2]) act ; (rr[j2] - CBIG x[j2]) act ]
   auto wood = [&](double* x, const double* rr) {
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       double Cc[64];
       for (int i = 0; i < m * m; ++i) Cc[i] = C[i];
       for (int a = 0; a < p; ++a) {
@@ -538,36 +723,35 @@ __device__ void primal_solve(const DevNet& n, const Sh& s, double* rp, double* d
       }
       dense_solve(Cc, y, m);
     }
-    __syncthreads();
-    for (int q = threadIdx.x; q < n.Nj; q += NT) {
+    gsync<NT>();
+    for (int q = tid; q < n.Nj; q += NT) {
       double acc = 0.0;
       for (int c = 0; c < m; ++c) acc += cols[(size_t)c * n.Nj + q] * y[c];
       x[q] = x[q] - acc;
     }
-    __syncthreads();
+    gsync<NT>();
   };
   wood(dH, rp);
-  double* row1 = actf + p;  // p
   for (int it = 0; it < 2; ++it) {
-    for (int q = threadIdx.x; q < n.Nj; q += NT) res[q] = amul_node(n, q, s.P, dH, s.emh, s.S);
-    __syncthreads();
-    if (threadIdx.x == 0)
+    for (int q = tid; q < n.Nj; q += NT) res[q] = amul_node(n, T, s, q, dH);
+    gsync<NT>();
+    if (tid == 0)
       for (int i = 0; i < p; ++i)
         row1[i] = res[n.pcv_j1[i]] + res[n.pcv_j2[i]] - kCBIG * dH[n.pcv_j2[i]];
-    __syncthreads();
-    for (int q = threadIdx.x; q < n.Nj; q += NT) res[q] = rp[q] - res[q];
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    gsync<NT>();
+    for (int q = tid; q < n.Nj; q += NT) res[q] = rp[q] - res[q];
+    gsync<NT>();
+    if (tid == 0) {
       for (int i = 0; i < p; ++i)
         if (actf[i] != 0.0) res[n.pcv_j1[i]] = rp[n.pcv_j1[i]] - row1[i];
       for (int i = 0; i < p; ++i)
         if (actf[i] != 0.0) res[n.pcv_j2[i]] = rp[n.pcv_j2[i]] - dH[n.pcv_j2[i]];
     }
-    __syncthreads();
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, res, sx, t, refine);
+    gsync<NT>();
+    solve_refined<NT>(n, T, s, res, -1, sx, t, refine);
     wood(sx, res);
-    for (int q = threadIdx.x; q < n.Nj; q += NT) dH[q] = dH[q] + sx[q];
-    __syncthreads();
+    for (int q = tid; q < n.Nj; q += NT) dH[q] = dH[q] + sx[q];
+    gsync<NT>();
   }
 }
 
@@ -584,58 +768,132 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
   s.V0 = (double*)take(8ull * n.Nj);
   s.V1 = (double*)take(8ull * n.Nj);
   s.V2 = (double*)take(8ull * n.Nj);
-  s.e = (double*)take(8ull * n.Nj);
-  s.emh = (double*)take(8ull * n.Nj);
+  s.em_e = (double*)take(8ull * n.emcap);
+  s.em_ke = (double*)take(8ull * n.emcap);
+  s.em_emh = (double*)take(8ull * n.emcap);
   s.hf = (double*)take(8ull * (n.Nf > 0 ? n.Nf : 1));
   s.xf = (double*)take(8ull * (n.nxf > 0 ? n.nxf : 1));
   s.red = (double*)take(8ull * 4 * 32);
   s.small = (double*)take(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
+  s.eslot = (int16_t*)take(2ull * n.Nj);
+  s.wcnt = (int*)take(4ull * 32);
+  s.flag = (int*)take(16);      // [0] factor verdict, [1] error, [2] emitter count
+  s.err = s.flag + 1;
   s.S = (int8_t*)take(n.L);
   return s;
 }
 
-// ---------------------------------------------------------------- forward kernel
+size_t smem_bytes(const DevNet& n) {
+  auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
+  size_t o = 0;
+  o += 3 * a16(8ull * n.L);
+  o += a16(8ull * n.nnzL);
+  o += 3 * a16(8ull * n.Nj);
+  o += 3 * a16(8ull * n.emcap);
+  o += a16(8ull * (n.Nf > 0 ? n.Nf : 1));
+  o += a16(8ull * (n.nxf > 0 ? n.nxf : 1));
+  o += a16(8ull * 4 * 32);
+  o += a16(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
+  o += a16(2ull * n.Nj);
+  o += a16(4ull * 32);
+  o += a16(16);
+  o += a16(n.L);
+  return o;
+}
+
+// Compact the scenario's emitters (junctions with a positive coefficient, as
+// given by val[jnode[p]] > 0) into slots in increasing elimination order:
+// eslot[p] = slot or -1, em_ke = coefficient, em_e = initial flow 1.0
+// (hydraul.c initial EmitterFlow).  Returns false when they exceed emcap.
 template <int NT>
-__global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) {
+__device__ bool build_emitters(const DevNet& n, const Sh& s, const double* val, int stride_node) {
+  const int tid = gtid<NT>(), lane = threadIdx.x & 31, warp = tid >> 5;
+  int total = 0;
+  bool over = false;
+  for (int base = 0; base < n.Nj; base += NT) {
+    const int p = base + tid;
+    double v = 0.0;
+    if (p < n.Nj) v = val[stride_node ? n.jnode[p] : p];
+    const bool em = p < n.Nj && v > 0.0;
+    const unsigned mask = __ballot_sync(0xffffffffu, em);
+    if (lane == 0) s.wcnt[warp] = __popc(mask);
+    gsync<NT>();
+    int off = total, sum = 0;
+    for (int w = 0; w < NT / 32; ++w) {
+      if (w < warp) off += s.wcnt[w];
+      sum += s.wcnt[w];
+    }
+    const int slot = off + __popc(mask & ((1u << lane) - 1u));
+    if (p < n.Nj) {
+      if (em && slot < n.emcap) {
+        s.eslot[p] = (int16_t)slot;
+        s.em_ke[slot] = v;
+        s.em_e[slot] = 1.0;
+        s.em_emh[slot] = 0.0;
+      } else {
+        s.eslot[p] = -1;
+        if (em) over = true;
+      }
+    }
+    total += sum;
+    gsync<NT>();
+  }
+  if (tid == 0) s.flag[2] = total < n.emcap ? total : n.emcap;
+  if (tid == 0) *s.err = 0;
+  return !gsync_or<NT>(over);
+}
+
+// ---------------------------------------------------------------- forward kernel
+template <int NT, int GR>
+__global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
+                                                        int state_bytes) {
+  const int groups = GR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int b = blockIdx.x;
-  Sh s = carve(n, smem_raw);
+  // stage the schedule tables once per CTA
+  for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
+    ((uint4*)smem_raw)[i] = n.stab[i];
+  __syncthreads();
+  const STab T = stab_view(n, smem_raw);
+  const int g = threadIdx.x / NT;
+  const int b = blockIdx.x * groups + g;
+  if (b >= a.B) return;  // a whole group; other groups use their own barrier
+  Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   const double* rrow = a.r + (long long)b * a.r_stride;
   const double* kerow = a.ke + (long long)b * a.ke_stride;
   const double* drow = a.d + (long long)b * n.N;
   const double* rhrow = a.rh + (long long)b * n.N;
-  for (int f = threadIdx.x; f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
-  for (int k = threadIdx.x; k < n.L; k += NT) {
+  for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
+  for (int k = gtid<NT>(); k < n.L; k += NT) {
     s.q[k] = n.q_init[k];
     s.S[k] = n.status0[k];
   }
-  for (int p = threadIdx.x; p < n.Nj; p += NT) s.e[p] = kerow[n.jnode[p]] > 0.0 ? 1.0 : 0.0;
-  __syncthreads();
+  gsync<NT>();
+  const bool em_ok = build_emitters<NT>(n, s, kerow, 1);
   const bool sm = a.sm != 0;
   const int maxtrials = sm ? a.max_iter + (n.extra_iter > 0 ? n.extra_iter : 0) : a.max_iter;
   int nextcheck = n.checkfreq;
   int iters = maxtrials + 1, info = WDS_INFO_UNCONVERGED;
   double relerr = 0.0;
-  for (int it = 1; it <= maxtrials; ++it) {
+  for (int it = 1; it <= (em_ok ? maxtrials : 0); ++it) {
     // ---- headloss coefficients
-    for (int k = threadIdx.x; k < n.L; k += NT) {
+    for (int k = gtid<NT>(); k < n.L; k += NT) {
       double P, Y;
       link_coef(n, k, s.q[k], s.S[k], rrow[k], false, P, Y);
       s.P[k] = P;
       s.Y[k] = Y;
     }
-    __syncthreads();
-    assemble_gga<NT>(n, s, kerow, drow);
-    if (!ldl_factor<NT>(n, s.W)) {
+    gsync<NT>();
+    assemble_gga<NT>(n, T, s, kerow, drow);
+    if (!factor<NT>(n, T, s)) {
       info = WDS_INFO_NOT_PD;
       iters = it;
       break;
     }
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, s.V0, s.V1, s.V2, a.refine);
+    solve_refined<NT>(n, T, s, s.V0, -1, s.V1, s.V2, a.refine);
     // ---- newflows (hydsolver.c:358-514 as restated in solver.py:3092-3110)
     double sums[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = threadIdx.x; k < n.L; k += NT) {
-      const double dh = head_of(n.e1[k], s.V1, s.hf) - head_of(n.e2[k], s.V1, s.hf);
+    for (int k = gtid<NT>(); k < n.L; k += NT) {
+      const double dh = head_of(T.e1[k], s.V1, s.hf) - head_of(T.e2[k], s.V1, s.hf);
       double dq = s.Y[k] - s.P[k] * dh;
       if ((n.flags[k] & WDS_F_CHP) && dq > s.q[k]) dq = s.q[k] / 2.0;
       const double qn = s.q[k] - dq;
@@ -643,14 +901,14 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
       sums[0] += fabs(dq);
       sums[1] += fabs(qn);
     }
-    for (int p = threadIdx.x; p < n.Nj; p += NT) {
-      const double ke = kerow[n.jnode[p]];
-      if (ke > 0.0) {
+    for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+      const int es = s.eslot[p];
+      if (es >= 0) {
         double hl, hg;
-        emitter_hl(n, s.e[p], ke, hl, hg);
+        emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
         const double dqe = (hl - (s.V1[p] - n.el[p])) / hg;
-        const double en = s.e[p] - dqe;
-        s.e[p] = en;
+        const double en = s.em_e[es] - dqe;
+        s.em_e[es] = en;
         sums[2] += fabs(dqe);
         sums[3] += fabs(en);
       }
@@ -668,9 +926,9 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
     }
     // ---- batched status machine (hydsolve, solver.py:3126-3179)
     bool vchg = false;
-    for (int i = threadIdx.x; i < n.npcv; i += NT) {
+    for (int i = gtid<NT>(); i < n.npcv; i += NT) {
       const int k = n.pcv_link[i];
-      const double h1 = head_of(n.e1[k], s.V1, s.hf), h2 = head_of(n.e2[k], s.V1, s.hf);
+      const double h1 = head_of(T.e1[k], s.V1, s.hf), h2 = head_of(T.e2[k], s.V1, s.hf);
       const double qk = s.q[k], hs = n.pcv_hset[i], ht = n.htol;
       const int sk = s.S[k];
       const double hml = n.pcv_km[i] * (qk * qk);
@@ -688,16 +946,16 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
       if (ns != sk) vchg = true;
       s.S[k] = (int8_t)ns;
     }
-    vchg = __syncthreads_or(vchg);
+    vchg = gsync_or<NT>(vchg);
     const bool conv = relerr <= a.hacc;
     const bool br_conv = conv && it <= a.max_iter;
     const bool br_per = !conv && it <= n.maxcheck && nextcheck == it;
     bool chg = false;
     if (br_conv || br_per) {
-      for (int k = threadIdx.x; k < n.L; k += NT) {
+      for (int k = gtid<NT>(); k < n.L; k += NT) {
         const int st0 = s.S[k];
         int st = (st0 == WDS_XHEAD || st0 == WDS_TEMPCLOSED) ? WDS_OPEN : st0;
-        const double dh = head_of(n.e1[k], s.V1, s.hf) - head_of(n.e2[k], s.V1, s.hf);
+        const double dh = head_of(T.e1[k], s.V1, s.hf) - head_of(T.e2[k], s.V1, s.hf);
         const double qk = s.q[k];
         if (n.kind[k] == WDS_KIND_CVPIPE) {  // cvstatus
           const bool rev = qk < -n.qtol;
@@ -728,7 +986,7 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
         if (st != st0) chg = true;
         s.S[k] = (int8_t)st;
       }
-      chg = __syncthreads_or(chg);
+      chg = gsync_or<NT>(chg);
     }
     const bool stat_change = br_conv && (chg || vchg);
     if (br_conv && stat_change) nextcheck = it + n.checkfreq;
@@ -739,92 +997,93 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
       break;
     }
   }
-  __syncthreads();
+  gsync<NT>();
   // junction heads of the GGA solution stay in V1
   double* Hs = w.scr + (size_t)b * w.nscr * n.Nj;  // global copy of heads for the polish
   if (a.polish >= 0 && info == 0) {
-    for (int p = threadIdx.x; p < n.Nj; p += NT) Hs[p] = s.V1[p];
-    __syncthreads();
+    for (int p = gtid<NT>(); p < n.Nj; p += NT) Hs[p] = s.V1[p];
+    gsync<NT>();
     double* rp = Hs + n.Nj;
     double* res = rp + n.Nj;
     double* sx = res + n.Nj;
-    double* cols = sx + n.Nj;
+    double* cols = sx + n.Nj;                          // 2p Woodbury columns
     // small buffer: C [4p^2], y [2p], actf [p], row1 [p], then r_prv [p]
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
     for (int step = 0; step <= a.polish; ++step) {
       adj_coeffs<NT>(n, s, rrow, kerow);
-      assemble_reduced<NT>(n, s);
-      if (!ldl_factor<NT>(n, s.W)) {
+      assemble_reduced<NT>(n, T, s);
+      if (!factor<NT>(n, T, s)) {
         info = WDS_INFO_NOT_PD;
         break;
       }
       if (step == a.polish) break;  // terminal factor: keep it
       // residuals (autodiff.py:1032-1050); r_l overwrites Y
-      for (int k = threadIdx.x; k < n.L; k += NT) {
+      for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double hl = s.P[k] != 0.0 ? s.Y[k] / s.P[k] : 0.0;
-        s.Y[k] = hl - (head_of(n.e1[k], Hs, s.hf) - head_of(n.e2[k], Hs, s.hf));
+        s.Y[k] = hl - (head_of(T.e1[k], Hs, s.hf) - head_of(T.e2[k], Hs, s.hf));
       }
       bool any_act = false;
-      for (int i = threadIdx.x; i < n.npcv; i += NT) {
+      for (int i = gtid<NT>(); i < n.npcv; i += NT) {
         const bool act = s.S[n.pcv_link[i]] == WDS_ACTIVE;
         rprv[i] = (Hs[n.pcv_j2[i]] - n.pcv_hset[i]) * (act ? 1.0 : 0.0);
         any_act |= act;
       }
-      any_act = __syncthreads_or(any_act);
-      for (int p = threadIdx.x; p < n.Nj; p += NT) {
-        const int a0 = n.inc_ptr[p], m = n.inc_split[p], z = n.inc_ptr[p + 1];
+      any_act = gsync_or<NT>(any_act);
+      for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+        const int a0 = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
         double mm = 0.0, bt = 0.0;
         for (int e = m; e < z; ++e) {
-          const int k = n.inc[e];
+          const int k = inc_link(T, e);
           mm += s.q[k];
           bt += s.P[k] * s.Y[k];
         }
         for (int e = a0; e < m; ++e) {
-          const int k = n.inc[e];
+          const int k = inc_link(T, e);
           mm += -s.q[k];
           bt += -(s.P[k] * s.Y[k]);
         }
-        const double ke = kerow[n.jnode[p]];
-        double re = 0.0;
-        if (ke > 0.0) {
+        const int es = s.eslot[p];
+        double re = 0.0, emh = 0.0;
+        if (es >= 0) {
           double hl, hg;
-          emitter_hl(n, s.e[p], ke, hl, hg);
+          emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
           re = hl - (Hs[p] - n.el[p]);
-          mm = mm - s.e[p];
+          mm = mm - s.em_e[es];
+          emh = s.em_emh[es];
         }
         mm = mm - drow[n.jnode[p]];
-        s.V0[p] = (mm - bt) + s.emh[p] * re;
+        s.V0[p] = (mm - bt) + emh * re;
       }
-      __syncthreads();
-      primal_solve<NT>(n, s, rp, s.V1, res, sx, cols, rprv, any_act, a.refine);
+      gsync<NT>();
+      primal_solve<NT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act, a.refine);
       // dq, de, state update
-      for (int k = threadIdx.x; k < n.L; k += NT) {
-        const double b1 = junc_of(n.e1[k], s.V1), b2 = junc_of(n.e2[k], s.V1);
+      for (int k = gtid<NT>(); k < n.L; k += NT) {
+        const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
         if (i >= 0 && s.S[k] == WDS_ACTIVE) {
           const int j2 = n.pcv_j2[i];
-          const double ab2 = amul_node(n, j2, s.P, s.V1, s.emh, s.S) - kCBIG * s.V1[j2] * 1.0;
+          const double ab2 = amul_node(n, T, s, j2, s.V1) - kCBIG * s.V1[j2] * 1.0;
           dq = s.V0[j2] - ab2;
         }
         s.q[k] = s.q[k] + dq;
       }
-      for (int p = threadIdx.x; p < n.Nj; p += NT) {
-        const double ke = kerow[n.jnode[p]];
-        if (ke > 0.0) {
+      for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+        const int es = s.eslot[p];
+        if (es >= 0) {
           double hl, hg;
-          emitter_hl(n, s.e[p], ke, hl, hg);
+          emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
           const double re = hl - (Hs[p] - n.el[p]);
-          s.e[p] = s.e[p] + (-re + s.V1[p]) / hg;
+          s.em_e[es] = s.em_e[es] + (-re + s.V1[p]) / hg;
         }
         Hs[p] = Hs[p] + s.V1[p];
       }
-      __syncthreads();
+      gsync<NT>();
     }
     if (info == 0) {  // store the terminal state for the adjoint
       double* Wt = w.W + (size_t)b * n.nnzL;
-      for (int t = threadIdx.x; t < n.nnzL; t += NT) Wt[t] = s.W[t];
-      for (int k = threadIdx.x; k < n.L; k += NT) {
+      for (int t = gtid<NT>(); t < n.nnzL; t += NT) Wt[t] = s.W[t];
+      for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double q = s.q[k];
         w.P[(size_t)b * n.L + k] = s.P[k];
         double dr = 0.0;
@@ -837,46 +1096,51 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
         }
         w.dr[(size_t)b * n.L + k] = dr;
       }
-      for (int p = threadIdx.x; p < n.Nj; p += NT) {
-        const double ke = kerow[n.jnode[p]];
-        double hge = 1.0, dke = 0.0;
-        if (ke > 0.0) {
+      for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+        const int es = s.eslot[p];
+        double hge = 1.0, dke = 0.0, emh = 0.0;
+        if (es >= 0) {
+          const double ke = s.em_ke[es], ee = s.em_e[es];
           double hl;
-          emitter_hl(n, s.e[p], ke, hl, hge);
-          const double ea = fabs(s.e[p]);
+          emitter_hl(n, ee, ke, hl, hge);
+          const double ea = fabs(ee);
           const double pw = pow(fmax(ea, 1e-30), n.qexp - 1.0);
           const double raw = n.qexp * fmax(ke, kCSMALL) * pw;
-          dke = (raw < n.rqtol || ke < kCSMALL) ? 0.0 : pw * s.e[p];
+          dke = (raw < n.rqtol || ke < kCSMALL) ? 0.0 : pw * ee;
+          emh = s.em_emh[es];
         }
-        w.emh[(size_t)b * n.Nj + p] = s.emh[p];
+        w.emh[(size_t)b * n.Nj + p] = emh;
         w.hge[(size_t)b * n.Nj + p] = hge;
         w.dke[(size_t)b * n.Nj + p] = dke;
       }
       const int pc = n.npcv > 0 ? n.npcv : 1;
-      for (int i = threadIdx.x; i < n.npcv; i += NT)
+      for (int i = gtid<NT>(); i < n.npcv; i += NT)
         w.act[(size_t)b * pc + i] = s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1 : 0;
     }
-    for (int p = threadIdx.x; p < n.Nj; p += NT) s.V1[p] = Hs[p];
-    __syncthreads();
+    for (int p = gtid<NT>(); p < n.Nj; p += NT) s.V1[p] = Hs[p];
+    gsync<NT>();
   }
-  if (threadIdx.x == 0) w.valid[b] = (a.polish >= 0 && info == 0) ? 1 : 0;
+  gsync<NT>();
+  if (!em_ok) info = WDS_INFO_EMITTER_CAP;
+  if (gtid<NT>() == 0) w.valid[b] = (a.polish >= 0 && info == 0) ? 1 : 0;
   // ---- outputs
   double* hrow = a.head + (size_t)b * n.N;
   double* erow = a.emit + (size_t)b * n.N;
-  for (int f = threadIdx.x; f < n.Nf; f += NT) {
+  for (int f = gtid<NT>(); f < n.Nf; f += NT) {
     hrow[n.fnode[f]] = s.hf[f];
     erow[n.fnode[f]] = 0.0;
   }
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
+  for (int p = gtid<NT>(); p < n.Nj; p += NT) {
     const int nd = n.jnode[p];
     hrow[nd] = s.V1[p];
-    erow[nd] = kerow[nd] > 0.0 ? s.e[p] : 0.0;
+    const int es = s.eslot[p];
+    erow[nd] = es >= 0 ? s.em_e[es] : 0.0;
   }
-  for (int k = threadIdx.x; k < n.L; k += NT) {
+  for (int k = gtid<NT>(); k < n.L; k += NT) {
     a.flow[(size_t)b * n.L + k] = s.q[k];
     a.status[(size_t)b * n.L + k] = s.S[k];
   }
-  if (threadIdx.x == 0) {
+  if (gtid<NT>() == 0) {
     a.iters[b] = iters;
     a.relerr[b] = relerr;
     a.info[b] = info;
@@ -886,108 +1150,120 @@ __global__ void __launch_bounds__(NT) k_forward(DevNet n, DevWork w, FwdArgs a) 
 // ---------------------------------------------------------------- adjoint kernel
 // Node adjoint with constraint rows (autodiff.py:1107-1154) and the
 // theta contraction (autodiff.py:1246-1312).
-template <int NT>
-__global__ void __launch_bounds__(NT) k_adjoint(DevNet n, DevWork w, AdjArgs a) {
+template <int NT, int GR>
+__global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
+                                                        int state_bytes) {
+  const int groups = GR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int b = blockIdx.x;
-  Sh s = carve(n, smem_raw);
-  if (!w.valid[b]) return;  // uniform per CTA
+  for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
+    ((uint4*)smem_raw)[i] = n.stab[i];
+  __syncthreads();
+  const STab T = stab_view(n, smem_raw);
+  const int g = threadIdx.x / NT;
+  const int b = blockIdx.x * groups + g;
+  if (b >= a.B) return;
+  Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  if (!w.valid[b]) return;  // uniform per group
   const double* Wt = w.W + (size_t)b * n.nnzL;
-  for (int t = threadIdx.x; t < n.nnzL; t += NT) s.W[t] = Wt[t];
-  for (int k = threadIdx.x; k < n.L; k += NT) s.P[k] = w.P[(size_t)b * n.L + k];
+  for (int t = gtid<NT>(); t < n.nnzL; t += NT) s.W[t] = Wt[t];
+  for (int k = gtid<NT>(); k < n.L; k += NT) s.P[k] = w.P[(size_t)b * n.L + k];
   const int pc = n.npcv > 0 ? n.npcv : 1;
   // status is only consulted for ACTIVE flags of PRVs
-  for (int k = threadIdx.x; k < n.L; k += NT) {
+  for (int k = gtid<NT>(); k < n.L; k += NT) {
     const int i = n.link_pcv[k];
     s.S[k] = (i >= 0 && w.act[(size_t)b * pc + i]) ? WDS_ACTIVE : WDS_OPEN;
   }
-  for (int p = threadIdx.x; p < n.Nj; p += NT) s.emh[p] = w.emh[(size_t)b * n.Nj + p];
-  __syncthreads();
+  gsync<NT>();
+  // emitter slots from the stored 1/hgrad (positive exactly at emitters)
+  build_emitters<NT>(n, s, w.emh + (size_t)b * n.Nj, 0);
+  for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+    const int es = s.eslot[p];
+    if (es >= 0) s.em_emh[es] = w.emh[(size_t)b * n.Nj + p];
+  }
+  gsync<NT>();
   const double* gH = a.gH + (size_t)b * n.N;
   const double* gQ = a.gQ + (size_t)b * n.L;
   const double* gE = a.gE + (size_t)b * n.N;
   // r = B^T P gQ - em gE / hge - gH
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
-    const int a0 = n.inc_ptr[p], m = n.inc_split[p], z = n.inc_ptr[p + 1];
+  for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+    const int a0 = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
     double acc = 0.0;
     for (int e = m; e < z; ++e) {
-      const int k = n.inc[e];
+      const int k = inc_link(T, e);
       acc += s.P[k] * gQ[k];
     }
     for (int e = a0; e < m; ++e) {
-      const int k = n.inc[e];
+      const int k = inc_link(T, e);
       acc += -(s.P[k] * gQ[k]);
     }
     const int nd = n.jnode[p];
-    s.V0[p] = (acc - s.emh[p] * gE[nd]) - gH[nd];
+    const int es = s.eslot[p];
+    s.V0[p] = (acc - (es >= 0 ? s.em_emh[es] : 0.0) * gE[nd]) - gH[nd];
   }
   bool any_act = false;
-  for (int i = threadIdx.x; i < n.npcv; i += NT) any_act |= s.S[n.pcv_link[i]] == WDS_ACTIVE;
-  any_act = __syncthreads_or(any_act);
+  for (int i = gtid<NT>(); i < n.npcv; i += NT) any_act |= s.S[n.pcv_link[i]] == WDS_ACTIVE;
+  any_act = gsync_or<NT>(any_act);
   double* lam = s.V1;
   double* t = s.V2;
   if (!any_act) {
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, s.V0, lam, t, 2);
+    solve_refined<NT>(n, T, s, s.V0, -1, lam, t, 2);
   } else {
     const int p = n.npcv;
     double* scr = w.scr + (size_t)b * w.nscr * n.Nj;
     double* r2 = scr;
     double* res = r2 + n.Nj;
     double* sx = res + n.Nj;
-    double* cols = sx + n.Nj;
+    double* cols = sx + n.Nj;                 // p Woodbury columns
     double* C = s.small;
     double* y = C + p * p;
     double* actf = y + p;
-    if (threadIdx.x == 0)
+    if (gtid<NT>() == 0)
       for (int i = 0; i < p; ++i) actf[i] = s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0;
-    for (int q = threadIdx.x; q < n.Nj; q += NT) r2[q] = s.V0[q];
-    __syncthreads();
-    if (threadIdx.x == 0)
+    for (int q = gtid<NT>(); q < n.Nj; q += NT) r2[q] = s.V0[q];
+    gsync<NT>();
+    if (gtid<NT>() == 0)
       for (int i = 0; i < p; ++i)
         if (actf[i] != 0.0) r2[n.pcv_j2[i]] = gQ[n.pcv_link[i]];
-    __syncthreads();
-    solve_refined<NT>(n, s.W, s.P, s.emh, s.S, r2, lam, t, 2);
-    for (int c = 0; c < p; ++c) {
-      for (int q = threadIdx.x; q < n.Nj; q += NT) res[q] = q == n.pcv_j2[c] ? 1.0 : 0.0;
-      __syncthreads();
-      solve_refined<NT>(n, s.W, s.P, s.emh, s.S, res, cols + (size_t)c * n.Nj, t, 2);
-    }
-    if (threadIdx.x == 0)
+    gsync<NT>();
+    solve_refined<NT>(n, T, s, r2, -1, lam, t, 2);
+    for (int c = 0; c < p; ++c)
+      solve_refined<NT>(n, T, s, nullptr, n.pcv_j2[c], cols + (size_t)c * n.Nj, t, 0);
+    if (gtid<NT>() == 0)
       for (int a0 = 0; a0 < p; ++a0)
         for (int c = 0; c < p; ++c) {
           const double cw = cols[(size_t)c * n.Nj + n.pcv_j2[a0]] - cols[(size_t)c * n.Nj + n.pcv_j1[a0]];
           C[a0 * p + c] = cw * actf[a0] * actf[c] + (a0 == c ? 1.0 - actf[a0] : 0.0);
         }
-    __syncthreads();
+    gsync<NT>();
     auto wood = [&](double* x, const double* rr) {
-      if (threadIdx.x == 0) {
+      if (gtid<NT>() == 0) {
         double Cc[64];
         for (int i = 0; i < p * p; ++i) Cc[i] = C[i];
         for (int a0 = 0; a0 < p; ++a0)
           y[a0] = (x[n.pcv_j2[a0]] - x[n.pcv_j1[a0]] - rr[n.pcv_j2[a0]]) * actf[a0];
         dense_solve(Cc, y, p);
       }
-      __syncthreads();
-      for (int q = threadIdx.x; q < n.Nj; q += NT) {
+      gsync<NT>();
+      for (int q = gtid<NT>(); q < n.Nj; q += NT) {
         double acc = 0.0;
         for (int c = 0; c < p; ++c) acc += cols[(size_t)c * n.Nj + q] * y[c];
         x[q] = x[q] - acc;
       }
-      __syncthreads();
+      gsync<NT>();
     };
     wood(lam, r2);
     for (int it = 0; it < 2; ++it) {
-      for (int q = threadIdx.x; q < n.Nj; q += NT) res[q] = r2[q] - amul_node(n, q, s.P, lam, s.emh, s.S);
-      __syncthreads();
-      if (threadIdx.x == 0)
+      for (int q = gtid<NT>(); q < n.Nj; q += NT) res[q] = r2[q] - amul_node(n, T, s, q, lam);
+      gsync<NT>();
+      if (gtid<NT>() == 0)
         for (int i = 0; i < p; ++i)
           if (actf[i] != 0.0)
             res[n.pcv_j2[i]] = r2[n.pcv_j2[i]] - (lam[n.pcv_j2[i]] - lam[n.pcv_j1[i]]);
-      __syncthreads();
-      solve_refined<NT>(n, s.W, s.P, s.emh, s.S, res, sx, t, 2);
+      gsync<NT>();
+      solve_refined<NT>(n, T, s, res, -1, sx, t, 2);
       wood(sx, res);
-      for (int q = threadIdx.x; q < n.Nj; q += NT) lam[q] = lam[q] + sx[q];
-      __syncthreads();
+      for (int q = gtid<NT>(); q < n.Nj; q += NT) lam[q] = lam[q] + sx[q];
+      gsync<NT>();
     }
   }
   // theta contraction
@@ -997,11 +1273,11 @@ __global__ void __launch_bounds__(NT) k_adjoint(DevNet n, DevWork w, AdjArgs a) 
   double* gr = a.gr + (size_t)b * n.L;
   const double* hge = w.hge + (size_t)b * n.Nj;
   const double* dke = w.dke + (size_t)b * n.Nj;
-  for (int p = threadIdx.x; p < n.Nj; p += NT) {
+  for (int p = gtid<NT>(); p < n.Nj; p += NT) {
     const int nd = n.jnode[p];
     gd[nd] = lam[p];
     double g = 0.0;
-    if (s.emh[p] != 0.0) {
+    if (s.eslot[p] >= 0) {
       const double lam_e = (gE[nd] + lam[p]) / hge[p];
       g = -(lam_e * dke[p]);
     }
@@ -1009,22 +1285,22 @@ __global__ void __launch_bounds__(NT) k_adjoint(DevNet n, DevWork w, AdjArgs a) 
     grh[nd] = 0.0;
   }
   const double* dr = w.dr + (size_t)b * n.L;
-  for (int k = threadIdx.x; k < n.L; k += NT) {
-    const double l1 = junc_of(n.e1[k], lam), l2 = junc_of(n.e2[k], lam);
+  for (int k = gtid<NT>(); k < n.L; k += NT) {
+    const double l1 = junc_of(T.e1[k], lam), l2 = junc_of(T.e2[k], lam);
     const double lam_l = s.P[k] * (gQ[k] - (l2 - l1));
     gr[k] = -(lam_l * dr[k]);
   }
-  for (int f = threadIdx.x; f < n.Nf; f += NT) {
+  for (int f = gtid<NT>(); f < n.Nf; f += NT) {
     const int nd = n.fnode[f];
     double acc = 0.0;
     for (int e = n.finc_ptr[f]; e < n.finc_split[f]; ++e) {
       const int k = n.finc[e];
-      const double l1 = junc_of(n.e1[k], lam), l2 = junc_of(n.e2[k], lam);
+      const double l1 = junc_of(T.e1[k], lam), l2 = junc_of(T.e2[k], lam);
       acc += s.P[k] * (gQ[k] - (l2 - l1));
     }
     for (int e = n.finc_split[f]; e < n.finc_ptr[f + 1]; ++e) {
       const int k = n.finc[e];
-      const double l1 = junc_of(n.e1[k], lam), l2 = junc_of(n.e2[k], lam);
+      const double l1 = junc_of(T.e1[k], lam), l2 = junc_of(T.e2[k], lam);
       acc += -(s.P[k] * (gQ[k] - (l2 - l1)));
     }
     grh[nd] = acc + gH[nd];
@@ -1033,38 +1309,28 @@ __global__ void __launch_bounds__(NT) k_adjoint(DevNet n, DevWork w, AdjArgs a) 
   }
 }
 
-size_t smem_bytes(const DevNet& n) {
-  auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
-  size_t o = 0;
-  o += 3 * a16(8ull * n.L);
-  o += a16(8ull * n.nnzL);
-  o += 5 * a16(8ull * n.Nj);
-  o += a16(8ull * (n.Nf > 0 ? n.Nf : 1));
-  o += a16(8ull * (n.nxf > 0 ? n.nxf : 1));
-  o += a16(8ull * 4 * 32);
-  o += a16(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
-  o += a16(n.L);
-  return o;
-}
-
 }  // namespace
 
-size_t forward_smem_bytes(const DevNet& n, int) { return smem_bytes(n); }
-size_t adjoint_smem_bytes(const DevNet& n, int) { return smem_bytes(n); }
+size_t state_smem_bytes(const DevNet& n) { return smem_bytes(n); }
 
-int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, size_t smem, int threads,
+int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
                    void* stream, std::string* err) {
   if (n.npcv > 4) {
     *err = "wds_forward: more than 4 status-machine PRVs is not supported by this build";
     return WDS_E_UNSUPPORTED;
   }
-  auto kern = k_forward<256>;
+  const int st = (int)smem_bytes(n);
+  const size_t smem = (size_t)n.stab_bytes + (size_t)groups * st;
+  void (*kern)(DevNet, DevWork, FwdArgs, int) =
+      groups == 1 ? k_forward<256, 1> : groups == 2 ? k_forward<256, 2> : groups == 3 ? k_forward<256, 3>
+                                                                             : k_forward<256, 4>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
-  kern<<<a.B, 256, smem, (cudaStream_t)stream>>>(n, w, a);
+  const int grid = (a.B + groups - 1) / groups;
+  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward launch: ") + cudaGetErrorString(ce);
@@ -1073,19 +1339,24 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, size_t s
   return WDS_OK;
 }
 
-int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, size_t smem, int threads,
+int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int groups,
                    void* stream, std::string* err) {
   if (n.npcv > 4) {
     *err = "wds_adjoint: more than 4 status-machine PRVs is not supported by this build";
     return WDS_E_UNSUPPORTED;
   }
-  auto kern = k_adjoint<256>;
+  const int st = (int)smem_bytes(n);
+  const size_t smem = (size_t)n.stab_bytes + (size_t)groups * st;
+  void (*kern)(DevNet, DevWork, AdjArgs, int) =
+      groups == 1 ? k_adjoint<256, 1> : groups == 2 ? k_adjoint<256, 2> : groups == 3 ? k_adjoint<256, 3>
+                                                                             : k_adjoint<256, 4>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_adjoint: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
-  kern<<<a.B, 256, smem, (cudaStream_t)stream>>>(n, w, a);
+  const int grid = (a.B + groups - 1) / groups;
+  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) {
     *err = std::string("wds_adjoint launch: ") + cudaGetErrorString(ce);

@@ -89,6 +89,7 @@ struct WdsPlan {
   void* dwork = nullptr;
   int max_batch = 0;
   int threads = 256;
+  int groups = 1;
   size_t smem_fwd = 0, smem_adj = 0;
   int nnzA_lower = 0;
   bool have_state = false;
@@ -209,14 +210,18 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   std::vector<std::vector<int>> rows(Nj);
   for (int k = 0; k < Nj; ++k)
     for (int i : cstruct[k]) rows[i].push_back(k);
-  std::vector<int> rptr(Nj + 1, 0), rslot, rcol;
-  for (int j = 0; j < Nj; ++j) {
-    for (int k : rows[j]) {
-      rslot.push_back(slot(j, k));
-      rcol.push_back(k);
-    }
-    rptr[j + 1] = (int)rcol.size();
+  // forward-substitution items in level order: {j, first row entry, end, diag slot};
+  // row entries {slot of L_jk, k} stored contiguously in the same order
+  std::vector<int2> rent;
+  std::vector<int4> fitem(Nj), bitem(Nj);
+  for (int t = 0; t < Nj; ++t) {
+    int j = levcol[t];
+    int e0 = (int)rent.size();
+    for (int k : rows[j]) rent.push_back(make_int2(slot(j, k), k));
+    fitem[t] = make_int4(j, e0, (int)rent.size(), colptr[j]);
+    bitem[t] = make_int4(j, colptr[j], colptr[j + 1], 0);
   }
+  if (rent.empty()) rent.push_back(make_int2(0, 0));
   // factor tasks by level
   std::vector<int> ftask_ptr(nlev + 1, 0), fpair;
   std::vector<int4> ftask;
@@ -238,6 +243,37 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       }
     }
     ftask_ptr[l + 1] = (int)ftask.size();
+  }
+  // Execution mode per level and operation, one byte: bits 0-2 = log2 of the
+  // lane-group size G (each item's dot product is spread over G lanes and
+  // reduced with warp shuffles), bit 7 = wide (all 256 threads of the group,
+  // followed by a group barrier) instead of narrow (warp 0 only, __syncwarp).
+  // Cost model in units of one dependent round: rounds * (ceil(maxlen / G) +
+  // 0.6 log2 G + 1), plus 0.5 per group barrier.
+  auto pick_mode = [](int count, int maxlen) -> uint8_t {
+    double best = 1e30;
+    uint8_t mode = 0;
+    for (int wide = 0; wide <= 1; ++wide)
+      for (int lg = 0; lg <= 5; ++lg) {
+        const int G = 1 << lg, per = (wide ? 256 : 32) / G;
+        const double rounds = (double)((count + per - 1) / per);
+        const double cost = rounds * ((maxlen + G - 1) / G + 0.6 * lg + 1.0) + (wide ? 0.5 : 0.0);
+        if (cost < best - 1e-12) { best = cost; mode = (uint8_t)(lg | (wide ? 0x80 : 0)); }
+      }
+    return mode;
+  };
+  std::vector<uint8_t> md_fac(nlev), md_fwd(nlev), md_bwd(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    int mf = 0, mr = 0, mc = 0;
+    for (int t = ftask_ptr[l]; t < ftask_ptr[l + 1]; ++t) mf = std::max(mf, ftask[t].z - ftask[t].y);
+    for (int t = levptr[l]; t < levptr[l + 1]; ++t) {
+      int j = levcol[t];
+      mr = std::max(mr, (int)rows[j].size());
+      mc = std::max(mc, colptr[j + 1] - colptr[j] - 1);
+    }
+    md_fac[l] = pick_mode(ftask_ptr[l + 1] - ftask_ptr[l], mf);
+    md_fwd[l] = pick_mode(levptr[l + 1] - levptr[l], mr);
+    md_bwd[l] = pick_mode(levptr[l + 1] - levptr[l], mc);
   }
   // ---- link end codes, incidence lists, pairs
   auto code = [&](int nd) { return jrow[nd] >= 0 ? iperm[jrow[nd]] : -(fix_idx[nd] + 1); };
@@ -364,8 +400,11 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int v : fpair) ok = ok && in(v, 0, nnzL);
     for (auto& t : ftask) ok = ok && in(t.x, 0, nnzL) && t.y >= 0 && t.y <= t.z &&
                              t.z <= (int)fpair.size() / 3;
-    for (int v : rslot) ok = ok && in(v, 0, nnzL);
-    for (int v : rcol) ok = ok && in(v, 0, Nj);
+    for (auto& r : rent) ok = ok && in(r.x, 0, nnzL) && in(r.y, 0, Nj);
+    for (int t = 0; t < Nj; ++t)
+      ok = ok && in(fitem[t].x, 0, Nj) && fitem[t].y >= 0 && fitem[t].y <= fitem[t].z &&
+           fitem[t].z <= (int)rent.size() && in(fitem[t].w, 0, nnzL) && in(bitem[t].x, 0, Nj) &&
+           bitem[t].y >= 0 && bitem[t].y < bitem[t].z && bitem[t].z <= nnzL;
     for (int v : cb_idx) ok = ok && in(v, 0, std::max(npcv, 1));
     for (int i = 0; i < npcv; ++i)
       ok = ok && in(pcv_j1[i], 0, Nj) && in(pcv_j2[i], 0, Nj) && in(pcv_off[i], 0, nnzL) &&
@@ -381,6 +420,73 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int f = 0; f < Nf; ++f) ok = ok && in(fnodes[f], 0, N);
     if (!ok) return fail(WDS_E_ARG, "wds_plan: internal table failed its bounds check");
   }
+  // ---- compact tables (16-bit indices) staged in shared memory once per CTA
+  if (nnzL >= 65536 || Nj >= 32768 || Nf >= 16384 || L >= 32768 ||
+      (int)fpair.size() / 3 >= 65536 || (int)rent.size() >= 65536 || (int)inc.size() >= 65536 ||
+      (int)pair_link.size() >= 65536 || N >= 65536 || (int)ftask.size() >= 65536)
+    return fail(WDS_E_UNSUPPORTED, "wds_plan: network too large for the shared-memory schedule");
+  // factor tasks in level order: slot | diagonal << 31, update-list begin | count << 16
+  std::vector<uint16_t> s_ftp(ftask_ptr.begin(), ftask_ptr.end());
+  std::vector<uint2> s_ft(ftask.size());
+  for (size_t t = 0; t < ftask.size(); ++t)
+    s_ft[t] = make_uint2((uint32_t)ftask[t].x | ((uint32_t)ftask[t].w << 31),
+                         (uint32_t)ftask[t].y | ((uint32_t)(ftask[t].z - ftask[t].y) << 16));
+  if (s_ft.empty()) s_ft.push_back(make_uint2(0u, 0u));
+  std::vector<uint16_t> s_fp(fpair.begin(), fpair.end());
+  if (s_fp.empty()) s_fp.push_back(0);
+  std::vector<uint16_t> s_cp(colptr.begin(), colptr.end()), s_ri(rowidx.begin(), rowidx.end());
+  std::vector<uint16_t> s_lp(levptr.begin(), levptr.end());
+  // substitution items in level order: forward {j | e0 << 16, e1 | diag slot << 16},
+  // backward {j | c0 << 16, c1}; row entries {slot | k << 16} in level order
+  std::vector<uint2> s_fi(Nj), s_bi(Nj);
+  for (int t = 0; t < Nj; ++t) {
+    s_fi[t] = make_uint2((uint32_t)fitem[t].x | ((uint32_t)fitem[t].y << 16),
+                         (uint32_t)fitem[t].z | ((uint32_t)fitem[t].w << 16));
+    s_bi[t] = make_uint2((uint32_t)bitem[t].x | ((uint32_t)bitem[t].y << 16), (uint32_t)bitem[t].z);
+  }
+  std::vector<uint32_t> s_re(rent.size());
+  for (size_t e = 0; e < rent.size(); ++e) s_re[e] = (uint32_t)rent[e].x | ((uint32_t)rent[e].y << 16);
+  std::vector<uint8_t> s_md;
+  s_md.insert(s_md.end(), md_fac.begin(), md_fac.end());
+  s_md.insert(s_md.end(), md_fwd.begin(), md_fwd.end());
+  s_md.insert(s_md.end(), md_bwd.begin(), md_bwd.end());
+  // incidence entries: link | PRV-with-setting << 16 | other end fixed << 17 | fixed index << 18
+  std::vector<uint16_t> s_ip(inc_ptr.begin(), inc_ptr.end()), s_is(inc_split.begin(), inc_split.end());
+  std::vector<uint32_t> s_in(inc.size());
+  for (int p = 0; p < Nj; ++p)
+    for (int e = inc_ptr[p]; e < inc_ptr[p + 1]; ++e) {
+      const int k = inc[e];
+      const int other = e < inc_split[p] ? e2[k] : e1[k];
+      uint32_t v = (uint32_t)k;
+      if (net->link_kind[k] == WDS_KIND_PRV) v |= 1u << 16;
+      if (other < 0) v |= (1u << 17) | ((uint32_t)(-other - 1) << 18);
+      s_in[e] = v;
+    }
+  if (s_in.empty()) s_in.push_back(0);
+  std::vector<int16_t> s_e1(e1.begin(), e1.end()), s_e2(e2.begin(), e2.end());
+  std::vector<uint16_t> s_pp(pair_ptr.begin(), pair_ptr.end()), s_ps(pair_slot.begin(), pair_slot.end());
+  std::vector<uint16_t> s_pl(pair_link.size());
+  for (size_t e = 0; e < pair_link.size(); ++e)
+    s_pl[e] = (uint16_t)(pair_link[e] | (net->link_kind[pair_link[e]] == WDS_KIND_PRV ? 0x8000 : 0));
+  if (s_pl.empty()) s_pl.push_back(0);
+  if (s_ps.empty()) s_ps.push_back(0);
+  std::vector<uint16_t> s_fl(fill_slot.begin(), fill_slot.end());
+  if (s_fl.empty()) s_fl.push_back(0);
+  Blob sblob;
+  auto sadd = [&](auto& v) {
+    size_t off = (sblob.bytes.size() + 15) / 16 * 16;
+    size_t nb = v.size() * sizeof(v[0]);
+    sblob.bytes.resize(off + nb);
+    if (nb) std::memcpy(sblob.bytes.data() + off, v.data(), nb);
+    return (int)off;
+  };
+  const int so_ftp = sadd(s_ftp), so_ft = sadd(s_ft), so_fp = sadd(s_fp), so_cp = sadd(s_cp),
+            so_ri = sadd(s_ri), so_lp = sadd(s_lp), so_fi = sadd(s_fi), so_bi = sadd(s_bi),
+            so_re = sadd(s_re), so_md = sadd(s_md), so_ip = sadd(s_ip), so_is = sadd(s_is),
+            so_in = sadd(s_in), so_e1 = sadd(s_e1), so_e2 = sadd(s_e2), so_pp = sadd(s_pp),
+            so_pl = sadd(s_pl), so_ps = sadd(s_ps), so_fl = sadd(s_fl);
+  sblob.bytes.resize((sblob.bytes.size() + 15) / 16 * 16);
+  std::vector<unsigned char> stab_bytes = sblob.bytes;
   // ---- upload
   Blob blob;
   size_t o_e1 = blob.add(e1), o_e2 = blob.add(e2), o_kind = blob.add(kind), o_flags = blob.add(flags),
@@ -396,12 +502,13 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
          o_pl = blob.add(pair_link), o_ps = blob.add(pair_slot), o_fs = blob.add(fill_slot),
          o_cp = blob.add(colptr), o_ri = blob.add(rowidx), o_lp = blob.add(levptr),
          o_lc = blob.add(levcol), o_ftp = blob.add(ftask_ptr), o_ft = blob.add(ftask),
-         o_fp = blob.add(fpair), o_rp = blob.add(rptr), o_rs = blob.add(rslot), o_rc = blob.add(rcol),
+         o_fp = blob.add(fpair), o_rent = blob.add(rent), o_fit = blob.add(fitem),
+         o_bit = blob.add(bitem),
          o_pcl = blob.add(pcv_link), o_pj1 = blob.add(pcv_j1), o_pj2 = blob.add(pcv_j2),
          o_poff = blob.add(pcv_off), o_pxf = blob.add(pcv_xf), o_phs = blob.add(pcv_hset),
          o_pkm = blob.add(pcv_km), o_tll = blob.add(tl_link), o_tlt = blob.add(tl_tank),
          o_tlo = blob.add(tl_other), o_tlq = blob.add(tl_qsign), o_tlx = blob.add(tl_hmax),
-         o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags);
+         o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags), o_stab = blob.add(stab_bytes);
   WdsPlan* plan = new WdsPlan();
   if (cudaMalloc(&plan->dtab, blob.bytes.size()) != cudaSuccess) {
     delete plan;
@@ -433,21 +540,43 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.pair_slot = P_(int, o_ps); d.fill_slot = P_(int, o_fs); d.colptr = P_(int, o_cp);
   d.rowidx = P_(int, o_ri); d.levptr = P_(int, o_lp); d.levcol = P_(int, o_lc);
   d.ftask_ptr = P_(int, o_ftp); d.ftask = P_(int4, o_ft); d.fpair = P_(int, o_fp);
-  d.rptr = P_(int, o_rp); d.rslot = P_(int, o_rs); d.rcol = P_(int, o_rc);
+  d.rent = P_(int2, o_rent); d.fitem = P_(int4, o_fit); d.bitem = P_(int4, o_bit);
   d.pcv_link = P_(int, o_pcl); d.pcv_j1 = P_(int, o_pj1); d.pcv_j2 = P_(int, o_pj2);
   d.pcv_off = P_(int, o_poff); d.pcv_xf = P_(int, o_pxf); d.pcv_hset = P_(double, o_phs);
   d.pcv_km = P_(double, o_pkm); d.tl_link = P_(int, o_tll); d.tl_tank = P_(int, o_tlt);
   d.tl_other = P_(int, o_tlo); d.tl_qsign = P_(double, o_tlq); d.tl_hmax = P_(double, o_tlx);
   d.tl_hmin = P_(double, o_tln); d.tl_flags = P_(uint8_t, o_tlf);
+  d.stab = P_(uint4, o_stab);
+  d.stab_bytes = (int)stab_bytes.size();
+  d.o_ftask_ptr = so_ftp; d.o_ftask = so_ft; d.o_fpair = so_fp; d.o_colptr = so_cp;
+  d.o_rowidx = so_ri; d.o_levptr = so_lp; d.o_fitem = so_fi; d.o_bitem = so_bi;
+  d.o_rent = so_re; d.o_mode = so_md; d.o_inc_ptr = so_ip; d.o_inc_split = so_is;
+  d.o_inc = so_in; d.o_e1 = so_e1; d.o_e2 = so_e2; d.o_pptr = so_pp; d.o_plink = so_pl;
+  d.o_pslot = so_ps; d.o_fill = so_fl;
 #undef P_
   d.hexp = net->hexp; d.qexp = net->qexp; d.rqtol = net->rqtol; d.htol = net->htol;
   d.qtol = net->qtol; d.ucf_flow = net->ucf_flow; d.ucf_head = net->ucf_head;
   d.checkfreq = net->checkfreq; d.maxcheck = net->maxcheck; d.extra_iter = net->extra_iter;
+  d.emcap = std::min(Nj, net->emitter_capacity > 0 ? net->emitter_capacity : 64);
   plan->nnzA_lower = Nj + (int)pair_slot.size();
   plan->threads = 256;
-  plan->smem_fwd = forward_smem_bytes(d, plan->threads);
-  plan->smem_adj = adjoint_smem_bytes(d, plan->threads);
-  if (plan->smem_fwd > 227 * 1024 || plan->smem_adj > 227 * 1024) {
+  // scenario groups per CTA: the count that keeps the most scenarios resident
+  // per SM (228 KB of shared memory per SM, 1 KB reserved per CTA)
+  {
+    const size_t st = state_smem_bytes(d);
+    int best_g = 0, best_res = 0;
+    for (int g = 1; g <= 4; ++g) {
+      size_t sm = (size_t)d.stab_bytes + g * st;
+      if (sm > 227 * 1024) break;
+      int ctas = (int)((228 * 1024) / (sm + 1024));
+      ctas = std::min(ctas, 2048 / (256 * g));
+      if (ctas * g > best_res) { best_res = ctas * g; best_g = g; }
+    }
+    plan->groups = best_g;
+    plan->smem_fwd = best_g ? (size_t)d.stab_bytes + best_g * st : (size_t)d.stab_bytes + st;
+    plan->smem_adj = plan->smem_fwd;
+  }
+  if (plan->groups == 0 || plan->smem_fwd > 227 * 1024) {
     cudaFree(plan->dtab);
     delete plan;
     return fail(WDS_E_UNSUPPORTED,
@@ -456,7 +585,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   // ---- workspace
   plan->max_batch = max_batch;
   DevWork& w = plan->dw;
-  w.nscr = 4 + 2 * std::max(npcv, 1);  // heads, rp, res, sx, 2p Woodbury columns
+  // heads, rp, res, sx, 2p Woodbury columns, 2p+1 per-warp temporaries
+  w.nscr = 5 + 4 * std::max(npcv, 1);
   const size_t B = (size_t)max_batch, pc = (size_t)std::max(npcv, 1);
   size_t bytes = 0;
   auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
@@ -485,7 +615,7 @@ extern "C" int wds_plan_stats(const WdsPlan* plan, int64_t* o) {
   if (!plan || !o) return fail(WDS_E_ARG, "wds_plan_stats: bad argument");
   o[0] = plan->dn.Nj; o[1] = plan->dn.nnzL; o[2] = plan->dn.nlev; o[3] = plan->dn.nfpair;
   o[4] = (int64_t)plan->smem_fwd; o[5] = plan->dn.npcv; o[6] = plan->nnzA_lower;
-  o[7] = plan->threads;
+  o[7] = plan->groups;
   return WDS_OK;
 }
 
@@ -521,7 +651,7 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
   a.relerr = relerr; a.info = info;
   std::string err;
-  int rc = launch_forward(plan->dn, plan->dw, a, plan->smem_fwd, plan->threads, stream, &err);
+  int rc = launch_forward(plan->dn, plan->dw, a, plan->groups, stream, &err);
   if (rc != WDS_OK) return fail(rc, err);
   plan->have_state = o->polish_steps >= 0;
   plan->state_batch = batch;
@@ -538,7 +668,7 @@ extern "C" int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH, const
     return fail(WDS_E_STATE, "wds_adjoint: no implicit forward of this batch size to differentiate");
   AdjArgs a{batch, gH, gQ, gE, gd, grh, gke, gr};
   std::string err;
-  int rc = launch_adjoint(plan->dn, plan->dw, a, plan->smem_adj, plan->threads, stream, &err);
+  int rc = launch_adjoint(plan->dn, plan->dw, a, plan->groups, stream, &err);
   if (rc != WDS_OK) return fail(rc, err);
   return WDS_OK;
 }

@@ -72,6 +72,7 @@ class _Plan:
         net.checkfreq, net.maxcheck = solver.checkfreq, solver.maxcheck
         net.extra_iter = solver.extra_iter
         net.perm = None if solver.perm is None else _ptr(solver.perm, ctypes.c_int32)
+        net.emitter_capacity = int(solver.emitter_capacity)
         with torch.cuda.device(self.device):
             _lib.check(lib.wds_plan(ctypes.byref(net), self.max_batch,
                                     ctypes.byref(self.handle)), "wds_plan")
@@ -81,7 +82,7 @@ class _Plan:
         _lib.check(self.lib.wds_plan_stats(self.handle, _ptr(o, ctypes.c_int64)),
                    "wds_plan_stats")
         keys = ("Nj", "nnz_L", "n_levels", "n_update_pairs", "smem_bytes",
-                "n_prv", "nnz_A_lower", "threads")
+                "n_prv", "nnz_A_lower", "groups_per_cta")
         return dict(zip(keys, (int(v) for v in o)))
 
     def symbolic(self):
@@ -108,6 +109,15 @@ class _Plan:
             self.free()
         except Exception:
             pass
+
+
+def _check_emitter_cap(solver, info):
+    cap = torch.nonzero(info & _lib.INFO_EMITTER_CAP).flatten()
+    if cap.numel():
+        raise ValueError(
+            "scenarios %s have more emitters (Ke > 0) than emitter_capacity=%d; "
+            "raise solver.emitter_capacity before the first solve"
+            % (cap.tolist()[:8], solver.emitter_capacity))
 
 
 class GGASolver:
@@ -146,6 +156,8 @@ class GGASolver:
         self.dtype = dtype
         self.net = net
         self.sm100_refine = 2
+        # emitters per scenario kept in shared memory (junctions with Ke > 0)
+        self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
         lt = np.asarray(net.link_type, dtype=np.int64)
         nt = np.asarray(net.node_type, dtype=np.int64)
         allowed = ({CVPIPE, PIPE, TCV, PUMP, PRV} if self.dense_status_machine
@@ -357,6 +369,20 @@ class GGASolver:
         self._n1, self._n2 = n1, n2
         self._lt = lt
 
+    # Optional launch timing: when `launch_events` is a list, every C-ABI
+    # launch appends (name, start_event, end_event) recorded on the launching
+    # stream around the call.
+    launch_events = None
+
+    def _event_pair(self, stream, name):
+        if self.launch_events is None:
+            return None
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        self.launch_events.append((name, e0, e1))
+        return e0, e1
+
     def plan(self, batch):
         """Plan (symbolic analysis + device tables + workspace) able to run
         `batch` scenarios; plans are kept per capacity."""
@@ -465,12 +491,16 @@ class GGASolver:
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        cur = torch.cuda.current_stream(dev)
+        stream = cur.cuda_stream
+        ev = self._event_pair(cur, "forward")
         _lib.check(p.lib.wds_forward(
             p.handle, B, ctypes.byref(o), d.data_ptr(), rh.data_ptr(), ke.data_ptr(),
             r.data_ptr(), head.data_ptr(), flow.data_ptr(), emit.data_ptr(),
             status.data_ptr(), iters.data_ptr(), relerr.data_ptr(), info.data_ptr(),
             ctypes.c_void_p(stream)), "wds_forward")
+        if ev is not None:
+            ev[1].record(cur)
         return dict(head=head, flow=flow, emit=emit, status=status, iters=iters,
                     relerr=relerr, info=info, plan=p)
 
@@ -495,6 +525,7 @@ class GGASolver:
         sm = bool(status_machine)
         o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1)
         info = o["info"]
+        _check_emitter_cap(self, info)
         bad = torch.nonzero(info & _lib.INFO_NOT_PD).flatten()
         if bad.numel():
             raise RuntimeError(
