@@ -232,6 +232,7 @@ def main():
     import torch.distributed as dist
     from wdsgpu_b200 import synth
     from wdsgpu_b200.autodiff import dr_dC, implicit_solve
+    from wdsgpu_b200.sharding import allreduce_batch_summed
     from wdsgpu_b200.solver import GGASolver
 
     dev = torch.device("cuda", local)
@@ -266,9 +267,7 @@ def main():
         loss = (h.index_select(1, sens) ** 2).sum()
         loss.backward()
         gR, gK = R.grad, KE.grad
-        if world > 1:
-            dist.all_reduce(gR)
-            dist.all_reduce(gK)
+        allreduce_batch_summed([gR, gK])
         gC = gR * dC
         return loss.detach(), D.grad, gC, gK
 
