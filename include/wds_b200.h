@@ -161,6 +161,25 @@ int wds_plan_stats(const WdsPlan* plan, int64_t* out8);
 int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
                       int32_t* rowidx, int32_t* parent, int32_t* level);
 
+/* Size of the fixed device array used by wds_forward_noalloc (64 MiB). */
+#define WDS_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Forward without allocation (no counterpart in the reference, which always
+ * allocates through torch).  Same arguments and results as wds_forward, but
+ * the per-scenario workspace lives in one fixed WDS_NOALLOC_SCRATCH_BYTES
+ * device array held by every GPU that loads the library, so the call never
+ * calls cudaMalloc: for solve loops that must not allocate, or that run
+ * inside stream capture.  A batch whose workspace exceeds the array is
+ * rejected with WDS_E_ARG.  The first call on a device looks up the array's
+ * device address and should come before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race and must be serialised.  The call
+ * does not prepare wds_adjoint. */
+int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const WdsForwardOpts* opts,
+                        const double* demand, const double* fixed_head,
+                        const double* ke, const double* r,
+                        double* head, double* flow, double* emitter, int8_t* status,
+                        int32_t* iters, double* relerr, int32_t* info, void* stream);
+
 /* Release the plan and its device memory. */
 int wds_free(WdsPlan* plan);
 

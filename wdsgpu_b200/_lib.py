@@ -23,7 +23,7 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
            -4: "unsupported network", -5: "no forward state"}
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
-           "wds_plan_symbolic", "wds_free", "wds_last_error")
+           "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc")
 
 
 class WdsNetwork(ctypes.Structure):
@@ -79,6 +79,8 @@ def load():
     lib.wds_plan.restype = ctypes.c_int
     lib.wds_forward.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(WdsForwardOpts)] + [vp] * 11 + [vp]
     lib.wds_forward.restype = ctypes.c_int
+    lib.wds_forward_noalloc.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(WdsForwardOpts)] + [vp] * 11 + [vp]
+    lib.wds_forward_noalloc.restype = ctypes.c_int
     lib.wds_adjoint.argtypes = [vp, ctypes.c_int32] + [vp] * 7 + [vp]
     lib.wds_adjoint.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]

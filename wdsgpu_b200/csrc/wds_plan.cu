@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <string>
 #include <vector>
@@ -678,5 +679,102 @@ extern "C" int wds_free(WdsPlan* plan) {
   if (plan->dtab) cudaFree(plan->dtab);
   if (plan->dwork) cudaFree(plan->dwork);
   delete plan;
+  return WDS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Forward without allocation.
+//
+// Some callers cannot call cudaMalloc when they solve: a control loop that
+// must not touch the allocator after start-up (real-time pressure management,
+// where an allocation can stall for milliseconds), code recorded into a CUDA
+// graph by stream capture (where cudaMalloc is not allowed), or a host
+// process whose device memory is owned by another allocator.  For them,
+// wds_forward_noalloc runs the same forward kernel as wds_forward, but its
+// per-scenario workspace (the polish's heads and Woodbury columns, the
+// terminal factor and coefficients) lives in the fixed array below instead of
+// the plan's workspace.  The array is WDS_NOALLOC_SCRATCH_BYTES (64 MiB) and
+// every GPU that loads this library holds it until the process exits.
+//
+// The kernel writes every word of the workspace it reads later in the same
+// call, so nothing needs clearing between calls; the array keeps the last
+// call's contents.  All calls share the one array: calls whose kernels
+// overlap on the GPU (different streams, or different host threads) race on
+// it and must be serialised by the caller.  A call does not prepare
+// wds_adjoint; the plan's own state is left as it was.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[WDS_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+// Device address of g_noalloc_scratch per device (host code cannot use the
+// symbol itself: on the host it is only a stand-in, not a device address).
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mu;
+
+int scratch_address(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return fail(WDS_E_CUDA, "wds_forward_noalloc: no current CUDA device");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (ce != cudaSuccess || !p)
+      return fail(WDS_E_CUDA, std::string("wds_forward_noalloc: cudaGetSymbolAddress: ") +
+                                  cudaGetErrorString(ce));
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return WDS_OK;
+}
+}  // namespace
+
+extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const WdsForwardOpts* o,
+                                   const double* demand, const double* fixed_head,
+                                   const double* ke, const double* r, double* head, double* flow,
+                                   double* emitter, int8_t* status, int32_t* iters,
+                                   double* relerr, int32_t* info, void* stream) {
+  using namespace wds;
+  if (!plan || !o || batch <= 0) return fail(WDS_E_ARG, "wds_forward_noalloc: bad argument");
+  if (!demand || !fixed_head || !ke || !r || !head || !flow || !emitter || !status || !iters ||
+      !relerr || !info)
+    return fail(WDS_E_ARG, "wds_forward_noalloc: null pointer");
+  if (o->max_iter <= 0 || !(o->accuracy > 0.0) || o->refine < 0)
+    return fail(WDS_E_ARG, "wds_forward_noalloc: bad options");
+  const DevNet& d = plan->dn;
+  // the plan's workspace layout, for `batch` scenarios, inside the fixed array
+  const size_t B = (size_t)batch, pc = (size_t)std::max(d.npcv, 1);
+  const int nscr = plan->dw.nscr;
+  size_t bytes = 0;
+  auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
+  const size_t ow = take(B * d.nnzL * 8), op = take(B * d.L * 8), odr = take(B * d.L * 8),
+               oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
+               oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4);
+  if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
+    const size_t per = bytes / B;
+    return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
+                               std::to_string(bytes) + " bytes of scratch, the fixed array holds " +
+                               std::to_string((size_t)WDS_NOALLOC_SCRATCH_BYTES) +
+                               " (at most " + std::to_string(WDS_NOALLOC_SCRATCH_BYTES / per) +
+                               " scenarios of this network)");
+  }
+  void* base = nullptr;
+  int rc = scratch_address(&base);
+  if (rc != WDS_OK) return rc;
+  unsigned char* wb = (unsigned char*)base;
+  DevWork w;
+  w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
+  w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
+  w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
+  w.nscr = nscr;
+  FwdArgs a{};
+  a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
+  a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
+  a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
+  a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
+  a.relerr = relerr; a.info = info;
+  std::string err;
+  rc = launch_forward(d, w, a, plan->groups, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
   return WDS_OK;
 }
