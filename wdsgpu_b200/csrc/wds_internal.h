@@ -91,8 +91,7 @@ struct DevNet {
   // once per CTA (see STabOff)
   const uint4* stab;
   int stab_bytes;
-  int o_ftask_ptr, o_ftask, o_fpair, o_colptr, o_rowidx, o_levptr, o_fitem, o_bitem, o_rent,
-      o_mode, o_inc_ptr, o_inc_split, o_inc, o_e1, o_e2, o_pptr, o_plink, o_pslot, o_fill;
+  int o_spair, o_fpair, o_colptr, o_rowidx, o_levptr, o_rptr, o_rent, o_mode, o_inc_ptr, o_inc_split, o_inc, o_e1, o_e2, o_pptr, o_plink, o_pslot, o_fill;
   int emcap;  // emitters per scenario held in shared memory
 };
 
@@ -106,6 +105,7 @@ struct DevWork {
   double* dke;    // [B][Nj]
   int8_t* act;    // [B][max(npcv,1)]
   double* scr;    // [B][nscr][Nj] scratch vectors
+  double* lk;     // [B][2][L] link flows q and Y of the forward
   int nscr;
   int* valid;     // [B] 1 when the terminal state is stored
 };

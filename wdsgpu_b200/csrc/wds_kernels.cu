@@ -46,15 +46,13 @@ struct Sh {
 
 // Shared-memory view of the compact tables (16-bit indices).
 struct STab {
-  const uint16_t* ftask_ptr;  // [nlev+1] factor tasks per level
-  const uint2* ftask;         // slot | diag << 31, update begin | count << 16
+  const uint32_t* spair;      // [nnzL] update list: begin | count << 16 | diagonal << 31
   const uint16_t* fpair;      // [3 * npairs] {slot L_ik, slot L_jk, slot 1/D_k}
   const uint16_t* colptr;     // [Nj+1]
   const uint16_t* rowidx;     // [nnzL]
-  const uint16_t* levptr;     // [nlev+1] columns per level
-  const uint2* fitem;         // forward: j | e0 << 16, e1 | diag slot << 16
-  const uint2* bitem;         // backward: j | c0 << 16, c1
-  const uint32_t* rent;       // row entries slot | k << 16, level order
+  const uint16_t* levptr;     // [nlev+1] columns of a level (columns numbered in level order)
+  const uint16_t* rptr;       // [Nj+1] row lists
+  const uint32_t* rent;       // row entries slot | k << 16
   const uint8_t* mfac;        // [nlev] mode: log2 G | wide << 7
   const uint8_t* mfwd;
   const uint8_t* mbwd;
@@ -71,14 +69,12 @@ struct STab {
 
 __device__ STab stab_view(const DevNet& n, const unsigned char* b) {
   STab t;
-  t.ftask_ptr = (const uint16_t*)(b + n.o_ftask_ptr);
-  t.ftask = (const uint2*)(b + n.o_ftask);
+  t.spair = (const uint32_t*)(b + n.o_spair);
   t.fpair = (const uint16_t*)(b + n.o_fpair);
   t.colptr = (const uint16_t*)(b + n.o_colptr);
   t.rowidx = (const uint16_t*)(b + n.o_rowidx);
   t.levptr = (const uint16_t*)(b + n.o_levptr);
-  t.fitem = (const uint2*)(b + n.o_fitem);
-  t.bitem = (const uint2*)(b + n.o_bitem);
+  t.rptr = (const uint16_t*)(b + n.o_rptr);
   t.rent = (const uint32_t*)(b + n.o_rent);
   t.mfac = (const uint8_t*)(b + n.o_mode);
   t.mfwd = t.mfac + n.nlev;
@@ -337,16 +333,16 @@ __device__ __forceinline__ double group_sum(double v, int lg) {
 // reducing its entry's update list with warp shuffles.
 __device__ __forceinline__ void fac_level(const STab& T, double* W, int lv, int lg, int t,
                                           int nthr, bool& bad) {
-  const int t0 = T.ftask_ptr[lv], t1 = T.ftask_ptr[lv + 1];
+  const int t0 = T.colptr[T.levptr[lv]], t1 = T.colptr[T.levptr[lv + 1]];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = t0; base < t1; base += per) {
-    const int it = base + (t >> lg);
-    const bool valid = it < t1;
-    uint2 tk = make_uint2(0u, 0u);
+    const int slot = base + (t >> lg);
+    const bool valid = slot < t1;
+    uint32_t sp = 0;
     double acc = 0.0;
     if (valid) {
-      tk = T.ftask[it];
-      const int pb = tk.y & 0xffff, pe = pb + (int)(tk.y >> 16);
+      sp = T.spair[slot];
+      const int pb = sp & 0xffff, pe = pb + (int)((sp >> 16) & 0x7fff);
       for (int pr = pb + li; pr < pe; pr += G) {
         const uint16_t* f = T.fpair + 3 * pr;
         acc += W[f[0]] * W[f[1]] * W[f[2]];
@@ -354,9 +350,8 @@ __device__ __forceinline__ void fac_level(const STab& T, double* W, int lv, int 
     }
     acc = group_sum(acc, lg);
     if (valid && li == 0) {
-      const int slot = tk.x & 0x7fffffff;
       const double w = W[slot] - acc;
-      if (tk.x >> 31) {
+      if (sp >> 31) {
         if (!(w > 0.0) || !isfinite(w)) bad = true;
         W[slot] = 1.0 / w;
       } else {
@@ -372,23 +367,18 @@ __device__ __forceinline__ void fwd_level(const STab& T, const double* W, double
   const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
-    const int it = base + (t >> lg);
-    const bool valid = it < c1;
-    uint2 fi = make_uint2(0u, 0u);
+    const int j = base + (t >> lg);
+    const bool valid = j < c1;
     double acc = 0.0;
     if (valid) {
-      fi = T.fitem[it];
-      const int e0 = fi.x >> 16, e1 = fi.y & 0xffff;
-      for (int e = e0 + li; e < e1; e += G) {
+      const int e1 = T.rptr[j + 1];
+      for (int e = T.rptr[j] + li; e < e1; e += G) {
         const uint32_t r = T.rent[e];
         acc += W[r & 0xffff] * v[r >> 16];
       }
     }
     acc = group_sum(acc, lg);
-    if (valid && li == 0) {
-      const int j = fi.x & 0xffff;
-      v[j] = (v[j] - acc) * W[fi.y >> 16];
-    }
+    if (valid && li == 0) v[j] = (v[j] - acc) * W[T.colptr[j]];
   }
 }
 
@@ -398,20 +388,17 @@ __device__ __forceinline__ void bwd_level(const STab& T, const double* W, double
   const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
-    const int it = base + (t >> lg);
-    const bool valid = it < c1;
-    uint2 bi = make_uint2(0u, 0u);
+    const int j = base + (t >> lg);
+    const bool valid = j < c1;
+    int cb = 0;
     double acc = 0.0;
     if (valid) {
-      bi = T.bitem[it];
-      const int cb = bi.x >> 16, ce = bi.y;
+      cb = T.colptr[j];
+      const int ce = T.colptr[j + 1];
       for (int e = cb + 1 + li; e < ce; e += G) acc += W[e] * v[T.rowidx[e]];
     }
     acc = group_sum(acc, lg);
-    if (valid && li == 0) {
-      const int j = bi.x & 0xffff;
-      v[j] = v[j] - W[bi.x >> 16] * acc;
-    }
+    if (valid && li == 0) v[j] = v[j] - W[cb] * acc;
   }
 }
 
@@ -697,6 +684,12 @@ __device__ void primal_solve(const DevNet& n, const STab& T, const Sh& s, double
   gsync<NT>();
   solve_refined<NT>(n, T, s, rp, -1, dH, t, refine);
   for (int c = 0; c < m; ++c) {
+    // columns of inactive valves meet y = 0 in the correction: zero, not solved
+    if (actf[c < p ? c : c - p] == 0.0) {
+      for (int q = tid; q < n.Nj; q += NT) cols[(size_t)c * n.Nj + q] = 0.0;
+      gsync<NT>();
+      continue;
+    }
     const int u = c < p ? n.pcv_j2[c] : n.pcv_j1[c - p];
     solve_refined<NT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
   }
@@ -761,9 +754,9 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
   Sh s;
   size_t o = 0;
   auto take = [&](size_t bytes) { unsigned char* p = base + o; o = al16(o + bytes); return p; };
-  s.q = (double*)take(8ull * n.L);
+  s.q = nullptr;  // link flows and Y live in the global workspace (set by the kernel)
+  s.Y = nullptr;
   s.P = (double*)take(8ull * n.L);
-  s.Y = (double*)take(8ull * n.L);
   s.W = (double*)take(8ull * n.nnzL);
   s.V0 = (double*)take(8ull * n.Nj);
   s.V1 = (double*)take(8ull * n.Nj);
@@ -786,7 +779,7 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
 size_t smem_bytes(const DevNet& n) {
   auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
   size_t o = 0;
-  o += 3 * a16(8ull * n.L);
+  o += a16(8ull * n.L);
   o += a16(8ull * n.nnzL);
   o += 3 * a16(8ull * n.Nj);
   o += 3 * a16(8ull * n.emcap);
@@ -858,6 +851,8 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
   const int b = blockIdx.x * groups + g;
   if (b >= a.B) return;  // a whole group; other groups use their own barrier
   Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  s.q = w.lk + (size_t)b * 2 * n.L;
+  s.Y = s.q + n.L;
   const double* rrow = a.r + (long long)b * a.r_stride;
   const double* kerow = a.ke + (long long)b * a.ke_stride;
   const double* drow = a.d + (long long)b * n.N;
@@ -1226,8 +1221,14 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
         if (actf[i] != 0.0) r2[n.pcv_j2[i]] = gQ[n.pcv_link[i]];
     gsync<NT>();
     solve_refined<NT>(n, T, s, r2, -1, lam, t, 2);
-    for (int c = 0; c < p; ++c)
+    for (int c = 0; c < p; ++c) {
+      if (actf[c] == 0.0) {  // meets y = 0 in the correction
+        for (int q = gtid<NT>(); q < n.Nj; q += NT) cols[(size_t)c * n.Nj + q] = 0.0;
+        gsync<NT>();
+        continue;
+      }
       solve_refined<NT>(n, T, s, nullptr, n.pcv_j2[c], cols + (size_t)c * n.Nj, t, 0);
+    }
     if (gtid<NT>() == 0)
       for (int a0 = 0; a0 < p; ++a0)
         for (int c = 0; c < p; ++c) {

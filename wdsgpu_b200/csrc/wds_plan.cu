@@ -153,60 +153,77 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     perm = min_degree(Nj, adj);
   }
   for (int p = 0; p < Nj; ++p) iperm[perm[p]] = p;
-  // ---- symbolic factorisation: struct(L_j) = A_{>j,j} U children \ {j}
-  std::vector<std::vector<int>> cstruct(Nj), children(Nj);
-  std::vector<int> parent(Nj, -1), level(Nj, 0), mark(Nj, -1);
-  for (int j = 0; j < Nj; ++j) {
-    std::vector<int>& s = cstruct[j];
-    mark[j] = j;
-    for (int u : adj[perm[j]]) {
-      int i = iperm[u];
-      if (i > j && mark[i] != j) {
-        mark[i] = j;
-        s.push_back(i);
-      }
-    }
-    int lv = 0;
-    for (int c : children[j]) {
-      lv = std::max(lv, level[c] + 1);
-      for (int i : cstruct[c])
-        if (i != j && mark[i] != j) {
+  // ---- symbolic factorisation: struct(L_j) = A_{>j,j} U children \ {j}.
+  // Two passes: the second renumbers the columns by elimination-tree level
+  // (a topological order, so the factor is the same up to labels) so that
+  // every level is a contiguous range of columns and of slots.
+  std::vector<std::vector<int>> cstruct, children;
+  std::vector<int> parent, level, mark, colptr, rowidx, levptr, levcol;
+  int nlev = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    cstruct.assign(Nj, {}); children.assign(Nj, {});
+    parent.assign(Nj, -1); level.assign(Nj, 0); mark.assign(Nj, -1);
+    for (int j = 0; j < Nj; ++j) {
+      std::vector<int>& s = cstruct[j];
+      mark[j] = j;
+      for (int u : adj[perm[j]]) {
+        int i = iperm[u];
+        if (i > j && mark[i] != j) {
           mark[i] = j;
           s.push_back(i);
         }
+      }
+      int lv = 0;
+      for (int c : children[j]) {
+        lv = std::max(lv, level[c] + 1);
+        for (int i : cstruct[c])
+          if (i != j && mark[i] != j) {
+            mark[i] = j;
+            s.push_back(i);
+          }
+      }
+      level[j] = lv;
+      std::sort(s.begin(), s.end());
+      if (!s.empty()) {
+        parent[j] = s[0];
+        children[s[0]].push_back(j);
+      }
     }
-    level[j] = lv;
-    std::sort(s.begin(), s.end());
-    if (!s.empty()) {
-      parent[j] = s[0];
-      children[s[0]].push_back(j);
+    colptr.assign(Nj + 1, 0); rowidx.clear();
+    for (int j = 0; j < Nj; ++j) colptr[j + 1] = colptr[j] + 1 + (int)cstruct[j].size();
+    const int nnzL = colptr[Nj];
+    rowidx.resize(nnzL);
+    for (int j = 0; j < Nj; ++j) {
+      rowidx[colptr[j]] = j;
+      for (size_t t = 0; t < cstruct[j].size(); ++t) rowidx[colptr[j] + 1 + t] = cstruct[j][t];
+    }
+    nlev = 0;
+    for (int j = 0; j < Nj; ++j) nlev = std::max(nlev, level[j] + 1);
+    levptr.assign(nlev + 1, 0); levcol.clear();
+    for (int j = 0; j < Nj; ++j) levptr[level[j] + 1]++;
+    for (int l = 0; l < nlev; ++l) levptr[l + 1] += levptr[l];
+    levcol.resize(Nj);
+    {
+      std::vector<int> pos(levptr.begin(), levptr.end() - 1);
+      for (int j = 0; j < Nj; ++j) levcol[pos[level[j]]++] = j;
+    }
+    if (pass == 0) {
+      std::vector<int> p2(Nj);
+      for (int t = 0; t < Nj; ++t) p2[t] = perm[levcol[t]];
+      perm = p2;
+      for (int p = 0; p < Nj; ++p) iperm[perm[p]] = p;
     }
   }
-  std::vector<int> colptr(Nj + 1, 0), rowidx;
-  for (int j = 0; j < Nj; ++j) colptr[j + 1] = colptr[j] + 1 + (int)cstruct[j].size();
   const int nnzL = colptr[Nj];
-  rowidx.resize(nnzL);
-  for (int j = 0; j < Nj; ++j) {
-    rowidx[colptr[j]] = j;
-    for (size_t t = 0; t < cstruct[j].size(); ++t) rowidx[colptr[j] + 1 + t] = cstruct[j][t];
-  }
-  auto slot = [&](int i, int j) -> int {  // i >= j
+  for (int t = 0; t < Nj; ++t)
+    if (levcol[t] != t) return fail(WDS_E_ARG, "wds_plan: internal error (level order)");
+  auto slot = [&](int i, int j) -> int {  // slot of L_ij, i >= j; -1 if structurally zero
     if (i == j) return colptr[j];
     auto b = rowidx.begin() + colptr[j] + 1, e = rowidx.begin() + colptr[j + 1];
     auto it = std::lower_bound(b, e, i);
     if (it == e || *it != i) return -1;
     return (int)(it - rowidx.begin());
   };
-  int nlev = 0;
-  for (int j = 0; j < Nj; ++j) nlev = std::max(nlev, level[j] + 1);
-  std::vector<int> levptr(nlev + 1, 0), levcol;
-  for (int j = 0; j < Nj; ++j) levptr[level[j] + 1]++;
-  for (int l = 0; l < nlev; ++l) levptr[l + 1] += levptr[l];
-  levcol.resize(Nj);
-  {
-    std::vector<int> pos(levptr.begin(), levptr.end() - 1);
-    for (int j = 0; j < Nj; ++j) levcol[pos[level[j]]++] = j;
-  }
   // row lists: rows[i] = { k < i : i in struct(k) } ascending
   std::vector<std::vector<int>> rows(Nj);
   for (int k = 0; k < Nj; ++k)
@@ -426,25 +443,25 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       (int)fpair.size() / 3 >= 65536 || (int)rent.size() >= 65536 || (int)inc.size() >= 65536 ||
       (int)pair_link.size() >= 65536 || N >= 65536 || (int)ftask.size() >= 65536)
     return fail(WDS_E_UNSUPPORTED, "wds_plan: network too large for the shared-memory schedule");
-  // factor tasks in level order: slot | diagonal << 31, update-list begin | count << 16
-  std::vector<uint16_t> s_ftp(ftask_ptr.begin(), ftask_ptr.end());
-  std::vector<uint2> s_ft(ftask.size());
-  for (size_t t = 0; t < ftask.size(); ++t)
-    s_ft[t] = make_uint2((uint32_t)ftask[t].x | ((uint32_t)ftask[t].w << 31),
-                         (uint32_t)ftask[t].y | ((uint32_t)(ftask[t].z - ftask[t].y) << 16));
-  if (s_ft.empty()) s_ft.push_back(make_uint2(0u, 0u));
+  // Columns are numbered in level order, so level l owns the columns
+  // [levptr[l], levptr[l+1]) and the slots [colptr[levptr[l]], colptr[levptr[l+1]]).
+  // update list of every entry of L, by slot: begin | count << 16 | diagonal << 31
+  std::vector<uint32_t> s_sp(nnzL, 0);
+  for (auto& t : ftask) {
+    if (t.z - t.y >= 32768) return fail(WDS_E_UNSUPPORTED, "wds_plan: update list too long");
+    s_sp[t.x] = (uint32_t)t.y | ((uint32_t)(t.z - t.y) << 16) | ((uint32_t)t.w << 31);
+  }
   std::vector<uint16_t> s_fp(fpair.begin(), fpair.end());
   if (s_fp.empty()) s_fp.push_back(0);
   std::vector<uint16_t> s_cp(colptr.begin(), colptr.end()), s_ri(rowidx.begin(), rowidx.end());
   std::vector<uint16_t> s_lp(levptr.begin(), levptr.end());
-  // substitution items in level order: forward {j | e0 << 16, e1 | diag slot << 16},
-  // backward {j | c0 << 16, c1}; row entries {slot | k << 16} in level order
-  std::vector<uint2> s_fi(Nj), s_bi(Nj);
-  for (int t = 0; t < Nj; ++t) {
-    s_fi[t] = make_uint2((uint32_t)fitem[t].x | ((uint32_t)fitem[t].y << 16),
-                         (uint32_t)fitem[t].z | ((uint32_t)fitem[t].w << 16));
-    s_bi[t] = make_uint2((uint32_t)bitem[t].x | ((uint32_t)bitem[t].y << 16), (uint32_t)bitem[t].z);
-  }
+  // row lists (forward substitution): entries {slot of L_jk | k << 16} of row j
+  // at [rptr[j], rptr[j+1])
+  std::vector<uint16_t> s_rp(Nj + 1, 0);
+  for (int j = 0; j < Nj; ++j) s_rp[j + 1] = (uint16_t)fitem[j].z;
+  for (int j = 0; j < Nj; ++j)
+    if (fitem[j].x != j || fitem[j].y != s_rp[j])
+      return fail(WDS_E_ARG, "wds_plan: internal error (row list order)");
   std::vector<uint32_t> s_re(rent.size());
   for (size_t e = 0; e < rent.size(); ++e) s_re[e] = (uint32_t)rent[e].x | ((uint32_t)rent[e].y << 16);
   std::vector<uint8_t> s_md;
@@ -481,9 +498,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     if (nb) std::memcpy(sblob.bytes.data() + off, v.data(), nb);
     return (int)off;
   };
-  const int so_ftp = sadd(s_ftp), so_ft = sadd(s_ft), so_fp = sadd(s_fp), so_cp = sadd(s_cp),
-            so_ri = sadd(s_ri), so_lp = sadd(s_lp), so_fi = sadd(s_fi), so_bi = sadd(s_bi),
-            so_re = sadd(s_re), so_md = sadd(s_md), so_ip = sadd(s_ip), so_is = sadd(s_is),
+  const int so_sp = sadd(s_sp), so_fp = sadd(s_fp), so_cp = sadd(s_cp),
+            so_ri = sadd(s_ri), so_lp = sadd(s_lp), so_rp = sadd(s_rp), so_re = sadd(s_re), so_md = sadd(s_md), so_ip = sadd(s_ip), so_is = sadd(s_is),
             so_in = sadd(s_in), so_e1 = sadd(s_e1), so_e2 = sadd(s_e2), so_pp = sadd(s_pp),
             so_pl = sadd(s_pl), so_ps = sadd(s_ps), so_fl = sadd(s_fl);
   sblob.bytes.resize((sblob.bytes.size() + 15) / 16 * 16);
@@ -549,8 +565,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.tl_hmin = P_(double, o_tln); d.tl_flags = P_(uint8_t, o_tlf);
   d.stab = P_(uint4, o_stab);
   d.stab_bytes = (int)stab_bytes.size();
-  d.o_ftask_ptr = so_ftp; d.o_ftask = so_ft; d.o_fpair = so_fp; d.o_colptr = so_cp;
-  d.o_rowidx = so_ri; d.o_levptr = so_lp; d.o_fitem = so_fi; d.o_bitem = so_bi;
+  d.o_spair = so_sp; d.o_fpair = so_fp; d.o_colptr = so_cp;
+  d.o_rowidx = so_ri; d.o_levptr = so_lp; d.o_rptr = so_rp;
   d.o_rent = so_re; d.o_mode = so_md; d.o_inc_ptr = so_ip; d.o_inc_split = so_is;
   d.o_inc = so_in; d.o_e1 = so_e1; d.o_e2 = so_e2; d.o_pptr = so_pp; d.o_plink = so_pl;
   d.o_pslot = so_ps; d.o_fill = so_fl;
@@ -593,7 +609,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
   size_t ow = take(B * nnzL * 8), op = take(B * L * 8), odr = take(B * L * 8),
          oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
-         oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4);
+         oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4),
+         olk = take(B * 2 * L * 8);
   if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
     cudaFree(plan->dtab);
     delete plan;
@@ -604,6 +621,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
+  w.lk = (double*)(wb + olk);
   // ---- host copy of the symbolic structure
   HostSym& hs = plan->sym;
   hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
@@ -749,7 +767,8 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
   const size_t ow = take(B * d.nnzL * 8), op = take(B * d.L * 8), odr = take(B * d.L * 8),
                oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
-               oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4);
+               oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4),
+               olk = take(B * 2 * d.L * 8);
   if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
     const size_t per = bytes / B;
     return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
@@ -766,6 +785,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
+  w.lk = (double*)(wb + olk);
   w.nscr = nscr;
   FwdArgs a{};
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
