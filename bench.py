@@ -357,7 +357,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "B": B, "network": "782 jn / 908 links",
+            "config": {"workload": WORKLOAD.replace("B=1024", "B=%d" % B), "B": B,
+                       "network": "782 jn / 908 links",
                        "l2": "flushed between steps (256 MB write, outside the timed events)",
                        "parallelism": "scenario shards per rank" if world > 1 else "single GPU",
                        "nnz_L": st["nnz_L"], "levels": st["n_levels"],
