@@ -13,6 +13,9 @@ constexpr double kCSMALL = 1e-6;   // hydcoeffs.c CSMALL, dgga/solver.py:34
 constexpr double kCBIG = 1e8;      // dgga/solver.py:35
 constexpr double kBIG = 1e10;
 constexpr double kQZERO = 1e-6;
+// Columns of the dense top block at most (16 x 16 threads x 3 x 3 entries each
+// hold the block in registers while it is inverted).
+constexpr int WDS_TOP_MAX = 48;
 
 // Device tables of one network.  Junction vectors are indexed by their
 // elimination index p (0..Nj-1); link ends are "end codes": p >= 0 for a
@@ -91,7 +94,10 @@ struct DevNet {
   // once per CTA (see STabOff)
   const uint4* stab;
   int stab_bytes;
-  int o_spair, o_fpair, o_colptr, o_rowidx, o_levptr, o_rptr, o_rent, o_mode, o_inc_ptr, o_inc_split, o_inc, o_e1, o_e2, o_pptr, o_plink, o_pslot, o_fill;
+  int o_spair, o_fpair, o_colptr, o_rowidx, o_levptr, o_rptr, o_rent, o_mode, o_inc_ptr, o_inc_split, o_inc, o_e1, o_e2, o_pptr, o_plink, o_pslot, o_fill, o_dslot;
+  // dense top block: levels [L0, nlev) = columns [cT, Nj), nT = Nj - cT
+  // (nT = 0 and L0 = nlev when the network has none)
+  int L0, cT, nT;
   int emcap;  // emitters per scenario held in shared memory
 };
 
@@ -106,6 +112,7 @@ struct DevWork {
   int8_t* act;    // [B][max(npcv,1)]
   double* scr;    // [B][nscr][Nj] scratch vectors
   double* lk;     // [B][2][L] link flows q and Y of the forward
+  double* M;      // [B][nT][nT] inverse of the top block's Schur complement
   int nscr;
   int* valid;     // [B] 1 when the terminal state is stored
 };

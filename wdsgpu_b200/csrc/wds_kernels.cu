@@ -40,6 +40,8 @@ struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
   double *em_e, *em_ke, *em_emh;  // per emitter slot: flow, coefficient, 1/hgrad
   int16_t* eslot;                 // [Nj] emitter slot of a junction or -1
+  double* tb;                     // [2][nT] pivot columns of the top-block inversion
+  double* Mg;                     // [nT][nT] top-block inverse (global workspace)
   int *wcnt, *flag, *err;
   int8_t* S;
 };
@@ -65,6 +67,7 @@ struct STab {
   const uint16_t* plink;      // link | PRV << 15
   const uint16_t* pslot;      // [npairs]
   const uint16_t* fill;       // [nfill]
+  const uint16_t* dslot;      // [nT (nT+1) / 2] slot of top-block entry (i >= j) or 0xffff
 };
 
 __device__ STab stab_view(const DevNet& n, const unsigned char* b) {
@@ -88,6 +91,7 @@ __device__ STab stab_view(const DevNet& n, const unsigned char* b) {
   t.plink = (const uint16_t*)(b + n.o_plink);
   t.pslot = (const uint16_t*)(b + n.o_pslot);
   t.fill = (const uint16_t*)(b + n.o_fill);
+  t.dslot = (const uint16_t*)(b + n.o_dslot);
   return t;
 }
 
@@ -328,12 +332,12 @@ __device__ __forceinline__ double group_sum(double v, int lg) {
   return v;
 }
 
-// One level of the left-looking LDL^T on `nthr` threads (thread index t):
-// the level's entries are split over lane groups of 1 << lg, each group
-// reducing its entry's update list with warp shuffles.
-__device__ __forceinline__ void fac_level(const STab& T, double* W, int lv, int lg, int t,
+// Factor slots [t0, t1) (one level, or the Schur-complement step of the top
+// block) on `nthr` threads (thread index t): the entries are split over lane
+// groups of 1 << lg, each group reducing its entry's update list with warp
+// shuffles.  Diagonal entries of factored columns become 1/D.
+__device__ __forceinline__ void fac_range(const STab& T, double* W, int t0, int t1, int lg, int t,
                                           int nthr, bool& bad) {
-  const int t0 = T.colptr[T.levptr[lv]], t1 = T.colptr[T.levptr[lv + 1]];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = t0; base < t1; base += per) {
     const int slot = base + (t >> lg);
@@ -361,10 +365,10 @@ __device__ __forceinline__ void fac_level(const STab& T, double* W, int lv, int 
   }
 }
 
-// One forward-substitution level: v_j = (v_j - sum_k L_jk D_k u_k) / D_j.
-__device__ __forceinline__ void fwd_level(const STab& T, const double* W, double* v, int lv,
-                                          int lg, int t, int nthr) {
-  const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
+// Forward substitution over rows [c0, c1): v_j = (v_j - sum_k L_jk D_k u_k) / D_j,
+// or, for the rows of the top block (top), v_j = v_j - sum over the lower columns.
+__device__ __forceinline__ void fwd_range(const STab& T, const double* W, double* v, int c0,
+                                          int c1, int lg, int t, int nthr, bool top) {
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
     const int j = base + (t >> lg);
@@ -378,7 +382,7 @@ __device__ __forceinline__ void fwd_level(const STab& T, const double* W, double
       }
     }
     acc = group_sum(acc, lg);
-    if (valid && li == 0) v[j] = (v[j] - acc) * W[T.colptr[j]];
+    if (valid && li == 0) v[j] = top ? v[j] - acc : (v[j] - acc) * W[T.colptr[j]];
   }
 }
 
@@ -402,50 +406,175 @@ __device__ __forceinline__ void bwd_level(const STab& T, const double* W, double
   }
 }
 
+// Inverse of the top block's Schur complement S (nT x nT, nT <= WDS_TOP_MAX)
+// by symmetric sweeps (Gauss-Jordan elimination without pivoting, in column
+// order; its pivots are the LDL^T pivots of S, positive for an SPD matrix):
+// sweeping k maps a_kk -> -1/p, a_ik -> a_ik/p, a_kj -> a_kj/p and
+// a_ij -> a_ij - a_ik a_kj / p (p = a_kk); after all nT sweeps the matrix
+// is -S^{-1}.  Thread (r, c) of a 16 x 16 grid keeps entries (r + 16 a,
+// c + 16 b), a, b < 3, in registers for all sweeps; the column of the next
+// pivot goes through shared memory (two alternating buffers, one barrier per
+// sweep).  S is read from the factor slots listed in dslot, S^{-1} is written
+// to Mg (row-major, full).  Returns 1 when this thread saw a pivot that was
+// not positive and finite.  Runs as a separate function so that its block of
+// registers does not add to the caller's.
+template <int NT>
+__device__ __noinline__ int top_inverse(const double* W, const uint16_t* dslot, double* tb,
+                                        double* Mg, int nT) {
+  static_assert(NT == 256, "the top-block inversion uses a 16 x 16 thread grid");
+  const int tid = gtid<NT>(), r = tid >> 4, c = tid & 15;
+  double a[3][3];
+#pragma unroll
+  for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+    for (int ib = 0; ib < 3; ++ib) {
+      const int i = r + 16 * ia, j = c + 16 * ib;
+      double x = 0.0;
+      if (i < nT && j < nT) {
+        const int hi = i > j ? i : j, lo = i > j ? j : i;
+        const int sl = dslot[hi * (hi + 1) / 2 + lo];
+        if (sl != 0xffff) x = W[sl];
+      }
+      a[ia][ib] = x;
+    }
+  if (c == 0)
+#pragma unroll
+    for (int ia = 0; ia < 3; ++ia)
+      if (r + 16 * ia < nT) tb[r + 16 * ia] = a[ia][0];
+  gsync<NT>();
+  int bad = 0;
+  for (int k = 0; k < nT; ++k) {
+    const double* cb = tb + (k & 1) * nT;
+    double* nb = tb + ((k + 1) & 1) * nT;
+    const double p = cb[k];
+    if (!(p > 0.0) || !isfinite(p)) bad = 1;
+    const double ip = 1.0 / p;
+    double ci[3], cj[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      ci[q] = r + 16 * q < nT ? cb[r + 16 * q] : 0.0;
+      cj[q] = c + 16 * q < nT ? cb[c + 16 * q] : 0.0;
+    }
+#pragma unroll
+    for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < 3; ++ib) {
+        const int i = r + 16 * ia, j = c + 16 * ib;
+        const double x = a[ia][ib];
+        a[ia][ib] = (i == k && j == k) ? -ip
+                    : (i == k || j == k) ? x * ip
+                                         : x - (ci[ia] * cj[ib]) * ip;
+      }
+    const int kn = k + 1;
+    if (kn < nT && c == (kn & 15)) {
+      const int ib = kn >> 4;
+#pragma unroll
+      for (int ia = 0; ia < 3; ++ia) {
+        const double x = ib == 0 ? a[ia][0] : ib == 1 ? a[ia][1] : a[ia][2];
+        if (r + 16 * ia < nT) nb[r + 16 * ia] = x;
+      }
+    }
+    gsync<NT>();
+  }
+#pragma unroll
+  for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+    for (int ib = 0; ib < 3; ++ib) {
+      const int i = r + 16 * ia, j = c + 16 * ib;
+      if (i < nT && j < nT) Mg[i * nT + j] = -a[ia][ib];
+    }
+  return bad;
+}
+
+// x_T = S^{-1} r_T for the top rows of v (vT = v + cT): row i of the product
+// on 4 lanes, each summing 12 or fewer terms; ends with a group barrier.
+template <int NT>
+__device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
+  const int tid = gtid<NT>(), i = tid >> 2, li = tid & 3;
+  double acc0 = 0.0, acc1 = 0.0;
+  if (i < nT) {
+    const double* row = Mg + i * nT;
+#pragma unroll
+    for (int q = 0; q < WDS_TOP_MAX / 4; q += 2) {
+      const int j0 = li + 4 * q, j1 = j0 + 4;
+      if (j0 < nT) acc0 += row[j0] * vT[j0];
+      if (j1 < nT) acc1 += row[j1] * vT[j1];
+    }
+  }
+  double acc = group_sum(acc0 + acc1, 2);
+  gsync<NT>();
+  if (i < nT && li == 0) vT[i] = acc;
+  gsync<NT>();
+}
+
 // Level-scheduled LDL^T.  Wide levels (many independent entries) use all the
 // group's threads and a group barrier; narrow levels run on warp 0 alone,
 // separated by __syncwarp.  W holds A on entry (pattern of L, fill zero) and
-// on exit the unscaled columns L_ij D_j with 1/D_j in the diagonal slot.
-// Returns true when every pivot was positive and finite.
+// on exit the unscaled columns L_ij D_j with 1/D_j in the diagonal slot, for
+// the columns below the top block; the top block's slots hold its Schur
+// complement and its inverse goes to s.Mg.  Returns true when every pivot was
+// positive and finite.
 template <int NT>
 __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
   const int tid = gtid<NT>();
   bool bad = false, prev_wide = true;
-  for (int lv = 0; lv < n.nlev; ++lv) {
+  for (int lv = 0; lv < n.L0; ++lv) {
     const int md = T.mfac[lv];
     const bool wide = (md & 0x80) != 0;
+    const int t0 = T.colptr[T.levptr[lv]], t1 = T.colptr[T.levptr[lv + 1]];
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      fac_level(T, s.W, lv, md & 7, tid, NT, bad);
+      fac_range(T, s.W, t0, t1, md & 7, tid, NT, bad);
       gsync<NT>();
     } else if (tid < 32) {
-      fac_level(T, s.W, lv, md & 7, tid, 32, bad);
+      fac_range(T, s.W, t0, t1, md & 7, tid, 32, bad);
       __syncwarp();
     }
     prev_wide = wide;
+  }
+  if (n.nT > 0) {
+    // Schur complement of the top block: its slots minus the lower columns' updates
+    const int md = T.mfac[n.L0];
+    const int t0 = T.colptr[n.cT];
+    if (!prev_wide) gsync<NT>();
+    if ((md & 0x80) || tid < 32)
+      fac_range(T, s.W, t0, n.nnzL, md & 7, tid, (md & 0x80) ? NT : 32, bad);
+    gsync<NT>();
+    if (top_inverse<NT>(s.W, T.dslot, s.tb, s.Mg, n.nT)) bad = true;
   }
   return !gsync_or<NT>(bad);
 }
 
-// In-place (L D L^T) v = b, level-scheduled in both sweeps.
+// In-place (L D L^T) v = b: forward levels below the top block, the top rows'
+// right-hand side, the dense top solve, backward levels below the top block.
 template <int NT>
 __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
   const int tid = gtid<NT>();
   bool prev_wide = true;
-  for (int lv = 0; lv < n.nlev; ++lv) {
+  for (int lv = 0; lv < n.L0; ++lv) {
     const int md = T.mfwd[lv];
     const bool wide = (md & 0x80) != 0;
+    const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      fwd_level(T, s.W, v, lv, md & 7, tid, NT);
+      fwd_range(T, s.W, v, c0, c1, md & 7, tid, NT, false);
       gsync<NT>();
     } else if (tid < 32) {
-      fwd_level(T, s.W, v, lv, md & 7, tid, 32);
+      fwd_range(T, s.W, v, c0, c1, md & 7, tid, 32, false);
       __syncwarp();
     }
     prev_wide = wide;
   }
-  for (int lv = n.nlev - 1; lv >= 0; --lv) {
+  if (n.nT > 0) {
+    const int md = T.mfwd[n.L0];
+    if (!prev_wide) gsync<NT>();
+    if ((md & 0x80) || tid < 32)
+      fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, tid, (md & 0x80) ? NT : 32, true);
+    gsync<NT>();
+    top_apply<NT>(s.Mg, v + n.cT, n.nT);
+    prev_wide = true;
+  }
+  for (int lv = n.L0 - 1; lv >= 0; --lv) {
     const int md = T.mbwd[lv];
     const bool wide = (md & 0x80) != 0;
     if (wide) {
@@ -769,6 +898,8 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
   s.red = (double*)take(8ull * 4 * 32);
   s.small = (double*)take(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
   s.eslot = (int16_t*)take(2ull * n.Nj);
+  s.tb = (double*)take(8ull * 2 * (n.nT > 0 ? n.nT : 1));
+  s.Mg = nullptr;  // set by the kernel
   s.wcnt = (int*)take(4ull * 32);
   s.flag = (int*)take(16);      // [0] factor verdict, [1] error, [2] emitter count
   s.err = s.flag + 1;
@@ -788,6 +919,7 @@ size_t smem_bytes(const DevNet& n) {
   o += a16(8ull * 4 * 32);
   o += a16(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
   o += a16(2ull * n.Nj);
+  o += a16(8ull * 2 * (n.nT > 0 ? n.nT : 1));
   o += a16(4ull * 32);
   o += a16(16);
   o += a16(n.L);
@@ -853,6 +985,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
   Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   s.q = w.lk + (size_t)b * 2 * n.L;
   s.Y = s.q + n.L;
+  s.Mg = w.M + (size_t)b * n.nT * n.nT;
   const double* rrow = a.r + (long long)b * a.r_stride;
   const double* kerow = a.ke + (long long)b * a.ke_stride;
   const double* drow = a.d + (long long)b * n.N;
@@ -1158,6 +1291,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
   const int b = blockIdx.x * groups + g;
   if (b >= a.B) return;
   Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  s.Mg = w.M + (size_t)b * n.nT * n.nT;  // terminal top-block inverse of the forward
   if (!w.valid[b]) return;  // uniform per group
   const double* Wt = w.W + (size_t)b * n.nnzL;
   for (int t = gtid<NT>(); t < n.nnzL; t += NT) s.W[t] = Wt[t];

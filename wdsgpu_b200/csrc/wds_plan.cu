@@ -217,6 +217,16 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   const int nnzL = colptr[Nj];
   for (int t = 0; t < Nj; ++t)
     if (levcol[t] != t) return fail(WDS_E_ARG, "wds_plan: internal error (level order)");
+  // ---- dense top block.  The top of the elimination tree is a thin chain
+  // (many levels, few columns).  The columns of the top levels [L0, nlev), at
+  // most WDS_TOP_MAX of them, are not factored column by column: their Schur
+  // complement S (updates from the columns below only) is inverted densely,
+  // and each substitution applies S^{-1} in one step instead of one step per
+  // level in each sweep.  Worth it from three top levels on.
+  int L0 = nlev;
+  for (int l = nlev - 1; l >= 0 && Nj - levptr[l] <= WDS_TOP_MAX; --l) L0 = l;
+  if (nlev - L0 < 3) L0 = nlev;
+  const int cT = levptr[L0], nT = Nj - cT;
   auto slot = [&](int i, int j) -> int {  // slot of L_ij, i >= j; -1 if structurally zero
     if (i == j) return colptr[j];
     auto b = rowidx.begin() + colptr[j] + 1, e = rowidx.begin() + colptr[j + 1];
@@ -224,10 +234,12 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     if (it == e || *it != i) return -1;
     return (int)(it - rowidx.begin());
   };
-  // row lists: rows[i] = { k < i : i in struct(k) } ascending
+  // row lists: rows[i] = { k < i : i in struct(k) } ascending; a top row keeps
+  // only its entries in the columns below the top block
   std::vector<std::vector<int>> rows(Nj);
   for (int k = 0; k < Nj; ++k)
-    for (int i : cstruct[k]) rows[i].push_back(k);
+    for (int i : cstruct[k])
+      if (i < cT || k < cT) rows[i].push_back(k);
   // forward-substitution items in level order: {j, first row entry, end, diag slot};
   // row entries {slot of L_jk, k} stored contiguously in the same order
   std::vector<int2> rent;
@@ -257,7 +269,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
           fpair.push_back(colptr[k]);
         }
         int pe = (int)fpair.size() / 3;
-        ftask.push_back(make_int4(e, pb, pe, i == j ? 1 : 0));
+        ftask.push_back(make_int4(e, pb, pe, (i == j && j < cT) ? 1 : 0));
       }
     }
     ftask_ptr[l + 1] = (int)ftask.size();
@@ -280,19 +292,32 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       }
     return mode;
   };
+  // Level L0 (when the top block exists) stands for all top levels: its
+  // factor mode is that of the Schur-complement step over every top slot, its
+  // forward mode that of the step that subtracts the lower columns from the
+  // top rows.
   std::vector<uint8_t> md_fac(nlev), md_fwd(nlev), md_bwd(nlev);
   for (int l = 0; l < nlev; ++l) {
+    const int l1 = l == L0 ? nlev : l + 1;
     int mf = 0, mr = 0, mc = 0;
-    for (int t = ftask_ptr[l]; t < ftask_ptr[l + 1]; ++t) mf = std::max(mf, ftask[t].z - ftask[t].y);
-    for (int t = levptr[l]; t < levptr[l + 1]; ++t) {
+    for (int t = ftask_ptr[l]; t < ftask_ptr[l1]; ++t) mf = std::max(mf, ftask[t].z - ftask[t].y);
+    for (int t = levptr[l]; t < levptr[l1]; ++t) {
       int j = levcol[t];
       mr = std::max(mr, (int)rows[j].size());
       mc = std::max(mc, colptr[j + 1] - colptr[j] - 1);
     }
-    md_fac[l] = pick_mode(ftask_ptr[l + 1] - ftask_ptr[l], mf);
-    md_fwd[l] = pick_mode(levptr[l + 1] - levptr[l], mr);
-    md_bwd[l] = pick_mode(levptr[l + 1] - levptr[l], mc);
+    md_fac[l] = pick_mode(ftask_ptr[l1] - ftask_ptr[l], mf);
+    md_fwd[l] = pick_mode(levptr[l1] - levptr[l], mr);
+    md_bwd[l] = pick_mode(levptr[l1] - levptr[l], mc);
+    if (l1 == nlev) break;
   }
+  // dense position (i, j), i >= j, of the top block -> slot of L, or 0xffff
+  std::vector<uint16_t> s_ds((size_t)std::max(nT * (nT + 1) / 2, 1), (uint16_t)0xffff);
+  for (int i = 0; i < nT; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const int sl = slot(cT + i, cT + j);
+      if (sl >= 0) s_ds[(size_t)i * (i + 1) / 2 + j] = (uint16_t)sl;
+    }
   // ---- link end codes, incidence lists, pairs
   auto code = [&](int nd) { return jrow[nd] >= 0 ? iperm[jrow[nd]] : -(fix_idx[nd] + 1); };
   std::vector<int> e1(L), e2(L);
@@ -423,6 +448,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       ok = ok && in(fitem[t].x, 0, Nj) && fitem[t].y >= 0 && fitem[t].y <= fitem[t].z &&
            fitem[t].z <= (int)rent.size() && in(fitem[t].w, 0, nnzL) && in(bitem[t].x, 0, Nj) &&
            bitem[t].y >= 0 && bitem[t].y < bitem[t].z && bitem[t].z <= nnzL;
+    for (uint16_t v : s_ds) ok = ok && (v == 0xffff || in(v, colptr[cT], nnzL));
+    ok = ok && nT >= 0 && nT <= WDS_TOP_MAX;
     for (int v : cb_idx) ok = ok && in(v, 0, std::max(npcv, 1));
     for (int i = 0; i < npcv; ++i)
       ok = ok && in(pcv_j1[i], 0, Nj) && in(pcv_j2[i], 0, Nj) && in(pcv_off[i], 0, nnzL) &&
@@ -501,7 +528,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   const int so_sp = sadd(s_sp), so_fp = sadd(s_fp), so_cp = sadd(s_cp),
             so_ri = sadd(s_ri), so_lp = sadd(s_lp), so_rp = sadd(s_rp), so_re = sadd(s_re), so_md = sadd(s_md), so_ip = sadd(s_ip), so_is = sadd(s_is),
             so_in = sadd(s_in), so_e1 = sadd(s_e1), so_e2 = sadd(s_e2), so_pp = sadd(s_pp),
-            so_pl = sadd(s_pl), so_ps = sadd(s_ps), so_fl = sadd(s_fl);
+            so_pl = sadd(s_pl), so_ps = sadd(s_ps), so_fl = sadd(s_fl), so_ds = sadd(s_ds);
   sblob.bytes.resize((sblob.bytes.size() + 15) / 16 * 16);
   std::vector<unsigned char> stab_bytes = sblob.bytes;
   // ---- upload
@@ -569,7 +596,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.o_rowidx = so_ri; d.o_levptr = so_lp; d.o_rptr = so_rp;
   d.o_rent = so_re; d.o_mode = so_md; d.o_inc_ptr = so_ip; d.o_inc_split = so_is;
   d.o_inc = so_in; d.o_e1 = so_e1; d.o_e2 = so_e2; d.o_pptr = so_pp; d.o_plink = so_pl;
-  d.o_pslot = so_ps; d.o_fill = so_fl;
+  d.o_pslot = so_ps; d.o_fill = so_fl; d.o_dslot = so_ds;
+  d.L0 = L0; d.cT = cT; d.nT = nT;
 #undef P_
   d.hexp = net->hexp; d.qexp = net->qexp; d.rqtol = net->rqtol; d.htol = net->htol;
   d.qtol = net->qtol; d.ucf_flow = net->ucf_flow; d.ucf_head = net->ucf_head;
@@ -610,7 +638,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   size_t ow = take(B * nnzL * 8), op = take(B * L * 8), odr = take(B * L * 8),
          oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
          oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4),
-         olk = take(B * 2 * L * 8);
+         olk = take(B * 2 * L * 8), otop = take(B * std::max(nT * nT, 1) * 8);
   if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
     cudaFree(plan->dtab);
     delete plan;
@@ -621,7 +649,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
-  w.lk = (double*)(wb + olk);
+  w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
   // ---- host copy of the symbolic structure
   HostSym& hs = plan->sym;
   hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
@@ -768,7 +796,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   const size_t ow = take(B * d.nnzL * 8), op = take(B * d.L * 8), odr = take(B * d.L * 8),
                oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
                oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4),
-               olk = take(B * 2 * d.L * 8);
+               olk = take(B * 2 * d.L * 8), otop = take(B * std::max(d.nT * d.nT, 1) * 8);
   if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
     const size_t per = bytes / B;
     return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
@@ -785,7 +813,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
-  w.lk = (double*)(wb + olk);
+  w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
   w.nscr = nscr;
   FwdArgs a{};
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
