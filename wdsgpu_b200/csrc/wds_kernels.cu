@@ -40,7 +40,7 @@ struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
   double *em_e, *em_ke, *em_emh;  // per emitter slot: flow, coefficient, 1/hgrad
   int16_t* eslot;                 // [Nj] emitter slot of a junction or -1
-  double* tb;                     // [2][nT] pivot columns of the top-block inversion
+  double* tb;                     // [2][49] pivot columns (+ 1/pivot) of the top-block inversion
   double* Mg;                     // [nT][nT] top-block inverse (global workspace)
   int *wcnt, *flag, *err;
   int8_t* S;
@@ -410,68 +410,102 @@ __device__ __forceinline__ void bwd_level(const STab& T, const double* W, double
 // by symmetric sweeps (Gauss-Jordan elimination without pivoting, in column
 // order; its pivots are the LDL^T pivots of S, positive for an SPD matrix):
 // sweeping k maps a_kk -> -1/p, a_ik -> a_ik/p, a_kj -> a_kj/p and
-// a_ij -> a_ij - a_ik a_kj / p (p = a_kk); after all nT sweeps the matrix
-// is -S^{-1}.  Thread (r, c) of a 16 x 16 grid keeps entries (r + 16 a,
-// c + 16 b), a, b < 3, in registers for all sweeps; the column of the next
-// pivot goes through shared memory (two alternating buffers, one barrier per
-// sweep).  S is read from the factor slots listed in dslot, S^{-1} is written
-// to Mg (row-major, full).  Returns 1 when this thread saw a pivot that was
-// not positive and finite.  Runs as a separate function so that its block of
-// registers does not add to the caller's.
+// a_ij -> a_ij - (a_ik/p) a_kj (p = a_kk); after all nT sweeps the matrix is
+// -S^{-1}.  The matrix stays symmetric, so only its lower triangle is kept:
+// thread (r, c) of a 16 x 16 grid holds entries (r + 16 a, c + 16 b),
+// b <= a < 3, in registers for all sweeps.  Column k+1 after sweep k goes
+// through shared memory: two alternating buffers of 49 (the column, zero
+// beyond nT, then 1/p of its pivot, which the pivot's owner computes and
+// checks); one group barrier per sweep.  Every entry takes the general update
+// without a test; the few lanes owning row or column k then overwrite those
+// entries.  S is read from the factor slots listed in dslot, S^{-1} is
+// written to Mg (row-major, both triangles).  Returns 1 when this thread
+// owned a pivot that was not positive and finite.  Runs as a separate
+// function so that its block of registers does not add to the caller's.
 template <int NT>
 __device__ __noinline__ int top_inverse(const double* W, const uint16_t* dslot, double* tb,
                                         double* Mg, int nT) {
-  static_assert(NT == 256, "the top-block inversion uses a 16 x 16 thread grid");
+  static_assert(NT == 256 && WDS_TOP_MAX == 48, "16 x 16 threads x 3 x 3 entries");
+  constexpr int ST = WDS_TOP_MAX + 1;
   const int tid = gtid<NT>(), r = tid >> 4, c = tid & 15;
   double a[3][3];
+  int bad = 0;
 #pragma unroll
   for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-    for (int ib = 0; ib < 3; ++ib) {
+    for (int ib = 0; ib <= ia; ++ib) {
       const int i = r + 16 * ia, j = c + 16 * ib;
       double x = 0.0;
-      if (i < nT && j < nT) {
-        const int hi = i > j ? i : j, lo = i > j ? j : i;
-        const int sl = dslot[hi * (hi + 1) / 2 + lo];
+      if (i < nT && j <= i) {
+        const int sl = dslot[i * (i + 1) / 2 + j];
         if (sl != 0xffff) x = W[sl];
       }
       a[ia][ib] = x;
     }
-  if (c == 0)
-#pragma unroll
-    for (int ia = 0; ia < 3; ++ia)
-      if (r + 16 * ia < nT) tb[r + 16 * ia] = a[ia][0];
+  // both buffers zero (rows beyond nT stay zero), then column 0 and 1/p of its pivot
+  if (tid < 2 * ST) tb[tid] = 0.0;
   gsync<NT>();
-  int bad = 0;
-  for (int k = 0; k < nT; ++k) {
-    const double* cb = tb + (k & 1) * nT;
-    double* nb = tb + ((k + 1) & 1) * nT;
-    const double p = cb[k];
-    if (!(p > 0.0) || !isfinite(p)) bad = 1;
-    const double ip = 1.0 / p;
-    double ci[3], cj[3];
+  if (c == 0) {
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      ci[q] = r + 16 * q < nT ? cb[r + 16 * q] : 0.0;
-      cj[q] = c + 16 * q < nT ? cb[c + 16 * q] : 0.0;
+    for (int ia = 0; ia < 3; ++ia) tb[r + 16 * ia] = a[ia][0];
+    if (r == 0) {
+      const double p = a[0][0];
+      if (!(p > 0.0) || !isfinite(p)) bad = 1;
+      tb[WDS_TOP_MAX] = __drcp_rn(p);
     }
+  }
+  gsync<NT>();
+#pragma unroll 1
+  for (int k = 0; k < nT; ++k) {
+    const double* cb = tb + (k & 1) * ST;
+    double* nb = tb + ((k + 1) & 1) * ST;
+    const double ip = cb[WDS_TOP_MAX];
+    const double c0 = cb[c], c1 = cb[c + 16], c2 = cb[c + 32];
+    const double t0 = cb[r] * ip, t1 = cb[r + 16] * ip, t2 = cb[r + 32] * ip;
+    a[0][0] = fma(-t0, c0, a[0][0]);
+    a[1][0] = fma(-t1, c0, a[1][0]);
+    a[1][1] = fma(-t1, c1, a[1][1]);
+    a[2][0] = fma(-t2, c0, a[2][0]);
+    a[2][1] = fma(-t2, c1, a[2][1]);
+    a[2][2] = fma(-t2, c2, a[2][2]);
+    const int km = k & 15, kb = k >> 4;
+    if (r == km || c == km) {  // entries in row k or column k
+      const double ti[3] = {t0, t1, t2}, cj[3] = {c0, c1, c2};
 #pragma unroll
-    for (int ia = 0; ia < 3; ++ia)
+      for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-      for (int ib = 0; ib < 3; ++ib) {
-        const int i = r + 16 * ia, j = c + 16 * ib;
-        const double x = a[ia][ib];
-        a[ia][ib] = (i == k && j == k) ? -ip
-                    : (i == k || j == k) ? x * ip
-                                         : x - (ci[ia] * cj[ib]) * ip;
-      }
+        for (int ib = 0; ib <= ia; ++ib) {
+          const bool ri = r == km && ia == kb, cj_ = c == km && ib == kb;
+          if (ri && cj_) a[ia][ib] = -ip;
+          else if (ri) a[ia][ib] = cj[ib] * ip;
+          else if (cj_) a[ia][ib] = ti[ia];
+        }
+    }
+    // publish column kn = k + 1: rows i >= kn from the owners of column kn,
+    // rows i < kn from the owners of row kn (a_{i,kn} = a_{kn,i})
     const int kn = k + 1;
-    if (kn < nT && c == (kn & 15)) {
-      const int ib = kn >> 4;
+    if (kn < nT) {
+      const int nm = kn & 15, nbk = kn >> 4;
+      if (c == nm) {
 #pragma unroll
-      for (int ia = 0; ia < 3; ++ia) {
-        const double x = ib == 0 ? a[ia][0] : ib == 1 ? a[ia][1] : a[ia][2];
-        if (r + 16 * ia < nT) nb[r + 16 * ia] = x;
+        for (int ia = 0; ia < 3; ++ia) {
+          const int i = r + 16 * ia;
+          if (ia >= nbk && i >= kn) {
+            const double x = nbk == 0 ? a[ia][0] : nbk == 1 ? a[ia][1] : a[ia][2];
+            nb[i] = x;
+            if (i == kn) {
+              if (!(x > 0.0) || !isfinite(x)) bad = 1;
+              nb[WDS_TOP_MAX] = __drcp_rn(x);
+            }
+          }
+        }
+      }
+      if (r == nm) {
+#pragma unroll
+        for (int ib = 0; ib < 3; ++ib) {
+          const int j = c + 16 * ib;
+          if (ib <= nbk && j < kn) nb[j] = nbk == 0 ? a[0][ib] : nbk == 1 ? a[1][ib] : a[2][ib];
+        }
       }
     }
     gsync<NT>();
@@ -479,9 +513,12 @@ __device__ __noinline__ int top_inverse(const double* W, const uint16_t* dslot, 
 #pragma unroll
   for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-    for (int ib = 0; ib < 3; ++ib) {
+    for (int ib = 0; ib <= ia; ++ib) {
       const int i = r + 16 * ia, j = c + 16 * ib;
-      if (i < nT && j < nT) Mg[i * nT + j] = -a[ia][ib];
+      if (i < nT && j <= i) {
+        Mg[i * nT + j] = -a[ia][ib];
+        Mg[j * nT + i] = -a[ia][ib];
+      }
     }
   return bad;
 }
@@ -516,7 +553,8 @@ __device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
 // positive and finite.
 template <int NT>
 __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
-  const int tid = gtid<NT>();
+  const int tid = gtid<NT>(), lane = tid & 31;
+  const bool inw = tid < 32;
   bool bad = false, prev_wide = true;
   for (int lv = 0; lv < n.L0; ++lv) {
     const int md = T.mfac[lv];
@@ -526,8 +564,8 @@ __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
       if (!prev_wide) gsync<NT>();
       fac_range(T, s.W, t0, t1, md & 7, tid, NT, bad);
       gsync<NT>();
-    } else if (tid < 32) {
-      fac_range(T, s.W, t0, t1, md & 7, tid, 32, bad);
+    } else if (inw) {
+      fac_range(T, s.W, t0, t1, md & 7, lane, 32, bad);
       __syncwarp();
     }
     prev_wide = wide;
@@ -537,8 +575,8 @@ __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
     const int md = T.mfac[n.L0];
     const int t0 = T.colptr[n.cT];
     if (!prev_wide) gsync<NT>();
-    if ((md & 0x80) || tid < 32)
-      fac_range(T, s.W, t0, n.nnzL, md & 7, tid, (md & 0x80) ? NT : 32, bad);
+    if (md & 0x80) fac_range(T, s.W, t0, n.nnzL, md & 7, tid, NT, bad);
+    else if (inw) fac_range(T, s.W, t0, n.nnzL, md & 7, lane, 32, bad);
     gsync<NT>();
     if (top_inverse<NT>(s.W, T.dslot, s.tb, s.Mg, n.nT)) bad = true;
   }
@@ -549,7 +587,8 @@ __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
 // right-hand side, the dense top solve, backward levels below the top block.
 template <int NT>
 __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
-  const int tid = gtid<NT>();
+  const int tid = gtid<NT>(), lane = tid & 31;
+  const bool inw = tid < 32;
   bool prev_wide = true;
   for (int lv = 0; lv < n.L0; ++lv) {
     const int md = T.mfwd[lv];
@@ -559,8 +598,8 @@ __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
       if (!prev_wide) gsync<NT>();
       fwd_range(T, s.W, v, c0, c1, md & 7, tid, NT, false);
       gsync<NT>();
-    } else if (tid < 32) {
-      fwd_range(T, s.W, v, c0, c1, md & 7, tid, 32, false);
+    } else if (inw) {
+      fwd_range(T, s.W, v, c0, c1, md & 7, lane, 32, false);
       __syncwarp();
     }
     prev_wide = wide;
@@ -568,8 +607,8 @@ __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
   if (n.nT > 0) {
     const int md = T.mfwd[n.L0];
     if (!prev_wide) gsync<NT>();
-    if ((md & 0x80) || tid < 32)
-      fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, tid, (md & 0x80) ? NT : 32, true);
+    if (md & 0x80) fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, tid, NT, true);
+    else if (inw) fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, lane, 32, true);
     gsync<NT>();
     top_apply<NT>(s.Mg, v + n.cT, n.nT);
     prev_wide = true;
@@ -581,8 +620,8 @@ __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
       if (!prev_wide) gsync<NT>();
       bwd_level(T, s.W, v, lv, md & 7, tid, NT);
       gsync<NT>();
-    } else if (tid < 32) {
-      bwd_level(T, s.W, v, lv, md & 7, tid, 32);
+    } else if (inw) {
+      bwd_level(T, s.W, v, lv, md & 7, lane, 32);
       __syncwarp();
     }
     prev_wide = wide;
@@ -898,7 +937,7 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
   s.red = (double*)take(8ull * 4 * 32);
   s.small = (double*)take(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
   s.eslot = (int16_t*)take(2ull * n.Nj);
-  s.tb = (double*)take(8ull * 2 * (n.nT > 0 ? n.nT : 1));
+  s.tb = (double*)take(8ull * 2 * (WDS_TOP_MAX + 1));
   s.Mg = nullptr;  // set by the kernel
   s.wcnt = (int*)take(4ull * 32);
   s.flag = (int*)take(16);      // [0] factor verdict, [1] error, [2] emitter count
@@ -919,7 +958,7 @@ size_t smem_bytes(const DevNet& n) {
   o += a16(8ull * 4 * 32);
   o += a16(8ull * (4 * n.npcv * n.npcv + 5 * n.npcv + 8));
   o += a16(2ull * n.Nj);
-  o += a16(8ull * 2 * (n.nT > 0 ? n.nT : 1));
+  o += a16(8ull * 2 * (WDS_TOP_MAX + 1));
   o += a16(4ull * 32);
   o += a16(16);
   o += a16(n.L);
