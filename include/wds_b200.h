@@ -121,6 +121,11 @@ typedef struct WdsForwardOpts {
   int32_t polish_steps;          /* reduced Newton polish steps; <0: plain solve only */
   int64_t ke_stride;             /* row stride of ke (0: one row for all)    */
   int64_t r_stride;              /* row stride of r  (0: one row for all)    */
+  /* Warm start (the q0 / e0 keywords of GGASolver.solve, dgga/solver.py:
+   * 2876-2887): device arrays or NULL for the defaults (q = initial flows,
+   * emitter flow 1 where Ke > 0). */
+  const double* q0;              /* [B,L] initial link flows, or NULL        */
+  const double* e0;              /* [B,N] initial emitter flows (read at junctions with Ke > 0), or NULL */
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;

@@ -456,8 +456,9 @@ class Model:
         return x
 
     def solve(self, d, rh, ke=None, r=None, accuracy=None, max_iter=None,
-              status_machine=False):
-        """Batched steady solve (restates solver.py:2703-3212)."""
+              status_machine=False, q0=None, e0=None):
+        """Batched steady solve (restates solver.py:2703-3212); q0 [B or 1, L]
+        and e0 [B or 1, N] are the warm start of solver.py:2876-2887."""
         d = np.atleast_2d(np.asarray(d, dtype=np.float64))
         B = d.shape[0]
         rh = np.broadcast_to(np.atleast_2d(rh), (B, self.N))
@@ -469,8 +470,13 @@ class Model:
         has_em = ke_j > 0.0
         max_iter = self.max_iter_default if max_iter is None else int(max_iter)
         hacc = self.hacc_default if accuracy is None else float(accuracy)
-        q = np.broadcast_to(self.init_flow(), (B, self.L)).copy()
-        e = np.where(has_em, 1.0, 0.0)
+        q0 = self.init_flow() if q0 is None else np.asarray(q0, dtype=np.float64)
+        q = np.broadcast_to(q0, (B, self.L)).copy()
+        if e0 is None:
+            e = np.where(has_em, 1.0, 0.0)
+        else:
+            e0 = np.broadcast_to(np.atleast_2d(np.asarray(e0, dtype=np.float64)), (B, self.N))
+            e = np.where(has_em, e0[:, self.junc], 0.0)
         H = np.array(rh, dtype=np.float64)
         H[:, self.junc] = 0.0
         if np.isnan(H[:, self.fixed]).any():
@@ -745,7 +751,7 @@ class Model:
         return gd, grh, gke, gr
 
     def implicit(self, d, rh, ke=None, r=None, accuracy=1e-12, max_iter=200,
-                 polish_steps=3, status_machine=True):
+                 polish_steps=3, status_machine=True, q0=None, e0=None):
         """Forward + polish; returns (out, state) where state feeds adjoint()."""
         d = np.atleast_2d(np.asarray(d, dtype=np.float64))
         B = d.shape[0]
@@ -754,7 +760,7 @@ class Model:
         r = self.r_hw if r is None else np.asarray(r, dtype=np.float64)
         r = np.broadcast_to(r, (B, self.L))
         out = self.solve(d, rh, ke=ke, r=r, accuracy=accuracy, max_iter=max_iter,
-                         status_machine=status_machine)
+                         status_machine=status_machine, q0=q0, e0=e0)
         if not out["converged"].all():
             raise RuntimeError("unconverged scenarios %s" %
                                np.flatnonzero(~out["converged"]).tolist())

@@ -15,7 +15,8 @@ and the reference outputs of
   * for small cases, implicit_solve(..., adjoint="cpu") on mode="epanet"
     (the EPANET-replica path with the scipy splu adjoint).
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py        (steady cases)
+        python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
 """
 import json
 import os
@@ -163,5 +164,64 @@ def main():
             os.path.getsize(path) // 1024))
 
 
+def make_eps(T=6):
+    """Extended-period pin: the reference's serial EPANET-replica EpsDriver
+    (dgga/eps.py) on a small pump/tank network, one scenario, T hourly frames.
+    The scenario's noisy diurnal demands are given to the reference as one
+    demand pattern per junction.  Tank mid-range heads come from a reference
+    steady solve with the tank nodes as zero-demand junctions."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    from wdsgpu_b200.net import JUNCTION, Net
+    dgga = _load_reference()
+    import dgga.eps
+    torch.set_default_dtype(torch.float64)
+    net0 = synth.eps_network(seed=7)
+    tn = np.asarray(net0.tank_node)
+    f = dict(net0.as_fields())
+    nt = np.asarray(f["node_type"]).copy()
+    nt[tn] = JUNCTION
+    jn = np.flatnonzero(nt == JUNCTION)
+    d0 = net0.demand_cfs_at(0)
+    empty = dict(tank_node=np.zeros(0, np.int32), tank_overflow=np.zeros(0, np.int8))
+    for k in ("tank_h0", "tank_hmin", "tank_hmax", "tank_area", "tank_vmin", "tank_v0",
+              "tank_vmax"):
+        empty[k] = np.zeros(0)
+    f.update(node_type=nt, dem_node=jn.astype(np.int32), dem_base_cfs=d0[jn],
+             dem_pat=np.full(jn.size, -1, np.int32), **empty)
+    pre = dgga.solver.GGASolver(dgga.parse.Net(**f), device="cpu", mode="dense",
+                                dense_status_machine=True)
+    o = pre.solve(torch.tensor(d0[None]), torch.tensor(np.nan_to_num(Net(**f).fixed_head_ft_at(0))[None]),
+                  status_machine=True, accuracy=1e-8, assemble="csr", linear_solver="dense")
+    centers = o["head_ft"][0].numpy()[tn]
+    net = synth.eps_network(seed=7, tank_center_ft=centers)
+    dem = synth.eps_demands(net, T, 1, seed=3)           # [T, 1, N] cfs
+    # one pattern per junction reproduces dem[t, 0, node] = base * factor[t]
+    fl = dict(net.as_fields())
+    junc = np.asarray(fl["dem_node"])
+    base = np.asarray(fl["dem_base_cfs"])
+    pats = [list(map(float, dem[:, 0, n] / b)) for n, b in zip(junc, base)]
+    fl.update(patterns=pats, pattern_ids=["p%d" % i for i in range(len(pats))],
+              dem_pat=np.arange(junc.size, dtype=np.int32))
+    meta = dict(fl["meta"])
+    meta.update(duration_sec=(T - 1) * 3600, hyd_step_sec=3600, pat_step_sec=3600,
+                report_step_sec=3600, pat_start_sec=0, tstart_sec=0, accuracy=1e-5)
+    fl["meta"] = meta
+    ref_net = dgga.parse.Net(**fl)
+    frames = dgga.eps.EpsDriver(ref_net).run()
+    blob = pack_net(net)
+    blob.update({"in_demand": dem, "in_T": np.array(T)})
+    for k in ("t_sec", "head_ft", "flow_int_cfs", "status", "iterations", "relerr"):
+        blob["ref_" + k] = np.asarray(frames[k])
+    path = os.path.join(HERE, "eps_ref.npz")
+    np.savez_compressed(path, **blob)
+    print("eps: frames at t=%s, iterations %s -> %s" % (
+        frames["t_sec"].tolist(), frames["iterations"].tolist(), os.path.basename(path)))
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["eps"]:
+        make_eps()
+    else:
+        main()

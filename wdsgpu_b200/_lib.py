@@ -57,7 +57,7 @@ class WdsForwardOpts(ctypes.Structure):
         ("accuracy", ctypes.c_double), ("max_iter", ctypes.c_int32),
         ("status_machine", ctypes.c_int32), ("refine", ctypes.c_int32),
         ("polish_steps", ctypes.c_int32), ("ke_stride", ctypes.c_int64),
-        ("r_stride", ctypes.c_int64),
+        ("r_stride", ctypes.c_int64), ("q0", ctypes.c_void_p), ("e0", ctypes.c_void_p),
     ]
 
 

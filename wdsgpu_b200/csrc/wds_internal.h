@@ -126,6 +126,8 @@ struct FwdArgs {
   const double* rh;
   const double* ke;
   const double* r;
+  const double* q0;  // [B][L] warm-start flows or null
+  const double* e0;  // [B][N] warm-start emitter flows or null
   double* head;
   double* flow;
   double* emit;

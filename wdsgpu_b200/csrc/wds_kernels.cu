@@ -1031,11 +1031,18 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
   const double* rhrow = a.rh + (long long)b * n.N;
   for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
   for (int k = gtid<NT>(); k < n.L; k += NT) {
-    s.q[k] = n.q_init[k];
+    s.q[k] = a.q0 ? a.q0[(size_t)b * n.L + k] : n.q_init[k];
     s.S[k] = n.status0[k];
   }
   gsync<NT>();
   const bool em_ok = build_emitters<NT>(n, s, kerow, 1);
+  if (a.e0) {  // warm start of the emitter flows (solver.py:2881-2887)
+    for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+      const int es = s.eslot[p];
+      if (es >= 0) s.em_e[es] = a.e0[(size_t)b * n.N + n.jnode[p]];
+    }
+    gsync<NT>();
+  }
   const bool sm = a.sm != 0;
   const int maxtrials = sm ? a.max_iter + (n.extra_iter > 0 ? n.extra_iter : 0) : a.max_iter;
   int nextcheck = n.checkfreq;

@@ -695,6 +695,7 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
   a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
   a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
+  a.q0 = o->q0; a.e0 = o->e0;
   a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
   a.relerr = relerr; a.info = info;
   std::string err;
@@ -819,6 +820,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
   a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
   a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
+  a.q0 = o->q0; a.e0 = o->e0;
   a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
   a.relerr = relerr; a.info = info;
   std::string err;

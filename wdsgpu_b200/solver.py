@@ -472,8 +472,10 @@ class GGASolver:
             raise NotImplementedError("record_schedule is not provided by the sm100 route")
 
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
-            refine=None, plan=None):
-        """One wds_forward call on device tensors; returns the raw outputs."""
+            refine=None, plan=None, q0=None, e0=None):
+        """One wds_forward call on device tensors; returns the raw outputs.
+        q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
+        warm start of GGASolver.solve (dgga/solver.py:2876-2887)."""
         p = plan or self.plan(B)
         dev = self.device
         head = torch.empty(B, self.N, dtype=torch.float64, device=dev)
@@ -491,6 +493,13 @@ class GGASolver:
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
+        for name, t, cols in (("q0", q0, self.L), ("e0", e0, self.N)):
+            if t is not None:
+                if (t.dtype != torch.float64 or t.device != dev or not t.is_contiguous()
+                        or tuple(t.shape) != (B, cols)):
+                    raise ValueError("%s must be a contiguous float64 [%d, %d] tensor on %s"
+                                     % (name, B, cols, dev))
+                setattr(o, name, t.data_ptr())
         cur = torch.cuda.current_stream(dev)
         stream = cur.cuda_stream
         ev = self._event_pair(cur, "forward")
@@ -517,13 +526,13 @@ class GGASolver:
         RuntimeError naming the scenarios."""
         self._guards(status_machine, assemble, linear_solver, link_status,
                      link_setting, record_schedule)
-        if q0 is not None or e0 is not None:
-            raise NotImplementedError("warm starts (q0/e0) are not provided by the sm100 route")
         d, rh, ke, r, B, single = self._inputs(demand_cfs, res_head_ft, ke_int, r_hw)
+        q0 = self._warm(q0, B, self.L)
+        e0 = self._warm(e0, B, self.N)
         max_iter = self.max_iter_default if max_iter is None else int(max_iter)
         hacc = self.hacc_default if accuracy is None else float(accuracy)
         sm = bool(status_machine)
-        o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1)
+        o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1, q0=q0, e0=e0)
         info = o["info"]
         _check_emitter_cap(self, info)
         bad = torch.nonzero(info & _lib.INFO_NOT_PD).flatten()
@@ -542,6 +551,19 @@ class GGASolver:
         if single:
             out = {k: v[0] for k, v in out.items()}
         return out
+
+    def _warm(self, x, B, cols):
+        """A 1-D or [B, cols] warm start as a contiguous [B, cols] FP64 device
+        tensor (the reference expands a 1-D q0/e0 over the batch,
+        solver.py:2878-2887)."""
+        if x is None:
+            return None
+        t = torch.as_tensor(x, dtype=torch.float64, device=self.device)
+        if t.dim() == 1:
+            t = t.unsqueeze(0).expand(B, -1)
+        if tuple(t.shape) != (B, cols):
+            raise ValueError("warm start must have shape [%d] or [%d, %d]" % (cols, B, cols))
+        return t.contiguous()
 
     # ------------------------------------------------------------ post checks
     def _check_pump_shutoff(self, H, q):

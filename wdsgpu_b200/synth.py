@@ -417,3 +417,123 @@ def feature_network(seed=5, n_junc=60, tank_level=0.5, with_chp=False):
         pump_qmax=np.full(npump, 1e10), pump_hmax=phmax,
         pump_upat=np.full(npump, -1, dtype=np.int32),
         pump_curve_q=cq, pump_curve_h=ch, pump_curve_ptr=ptr)
+
+
+def eps_network(seed=7, n_junc=60, n_pipes=75, n_pumps=4, n_tanks=3, res_head_m=10.0,
+                shutoff_m=(40.0, 60.0), tank_center_ft=None, tank_range_m=10.0,
+                tank_diam_m=(15.0, 30.0), base_lps=(0.05, 0.4), spacing_m=150.0):
+    """Extended-period network: one low reservoir feeding a looped network
+    through power-function pumps h = a - b q^1.85 (shutoff a in `shutoff_m`,
+    75 % of it at the design flow), and cylindrical tanks on junctions far
+    from the source, starting at mid-range.  Reservoir-incident links become
+    the pumps (parallel copies are added when there are fewer than
+    `n_pumps`; surplus ones are closed).  `tank_center_ft` gives each tank's
+    mid-range head (ft); the default is the reservoir head plus 60 % of the
+    mean shutoff head, a rough grade-line estimate."""
+    base = looped_network(seed, n_junc=n_junc + n_tanks, n_res=1, n_pipes=n_pipes,
+                          res_head_m=(res_head_m, res_head_m), base_lps=base_lps,
+                          spacing_m=spacing_m)
+    rng = np.random.default_rng(seed + 1000)
+    N = base.N
+    nt = base.node_type.copy()
+    res = int(np.flatnonzero(nt == RESERVOIR)[0])
+    n1 = list(base.link_n1.tolist())
+    n2 = list(base.link_n2.tolist())
+    ltype = list(base.link_type.tolist())
+    status = list(base.init_status.tolist())
+    diam, length, c = list(base.diam_ft), list(base.len_ft), list(base.roughness)
+    inc = [k for k in range(base.L) if n1[k] == res or n2[k] == res]
+    pumps = inc[:n_pumps]
+    for k in inc[n_pumps:]:
+        status[k] = 0                                   # surplus source links closed
+    while len(pumps) < n_pumps:                         # parallel copies
+        k0 = pumps[len(pumps) % max(len(inc), 1)]
+        n1.append(n1[k0]); n2.append(n2[k0]); ltype.append(PIPE); status.append(1)
+        diam.append(diam[k0]); length.append(0.0); c.append(0.0)
+        pumps.append(len(n1) - 1)
+    for k in pumps:
+        ltype[k] = PUMP
+        if n2[k] == res:                                # discharge away from the source
+            n1[k], n2[k] = n2[k], n1[k]
+        length[k] = 0.0
+        c[k] = 0.0
+        status[k] = 1
+    L = len(n1)
+    diam, length, c = np.asarray(diam), np.asarray(length), np.asarray(c)
+    # pump curves, internal units: h0 = -a (shutoff), r so that the head is 75 % of a
+    # at the design flow (the peak demand shared by the pumps)
+    d0 = base.demand_cfs_at(0)
+    q_design = 1.6 * float(d0.sum()) / n_pumps
+    a_ft = rng.uniform(*shutoff_m, n_pumps) / MperFT
+    nexp = 1.85
+    pr = 0.25 * a_ft / q_design ** nexp
+    # tanks: junctions far from the source, spread out (greedy farthest points)
+    pts_el = base.elev_ft
+    junc = np.flatnonzero(nt == JUNCTION)
+    dist = np.abs(junc - res).astype(np.float64)
+    chosen = [int(junc[np.argmax(dist)])]
+    while len(chosen) < n_tanks:
+        dd = np.min(np.abs(junc[:, None] - np.asarray(chosen)[None, :]), axis=1)
+        dd = np.minimum(dd, dist)
+        chosen.append(int(junc[np.argmax(dd)]))
+    tanks = np.asarray(chosen, dtype=np.int32)
+    nt[tanks] = TANK
+    if tank_center_ft is None:
+        tank_center_ft = np.full(n_tanks, res_head_m / MperFT + 0.6 * float(a_ft.mean()))
+    ctr = np.asarray(tank_center_ft, dtype=np.float64)
+    half = 0.5 * tank_range_m / MperFT
+    hmin, hmax = ctr - half, ctr + half
+    el = pts_el.copy()
+    el[tanks] = hmin
+    area = np.pi * (rng.uniform(*tank_diam_m, n_tanks) / MperFT) ** 2 / 4.0
+    h0 = 0.5 * (hmin + hmax)
+    junc2 = np.flatnonzero(nt == JUNCTION)
+    r = _r_hw(length, c, diam)
+    ltype = np.asarray(ltype, dtype=np.int8)
+    setting = np.zeros(L)
+    setting[pumps] = 1.0
+    return Net(
+        node_id=base.node_id, node_type=nt, elev_ft=el, node_ke=np.zeros(N),
+        res_head_pat=base.res_head_pat, link_id=[f"l{k}" for k in range(L)],
+        link_type=ltype, link_n1=np.asarray(n1, dtype=np.int32),
+        link_n2=np.asarray(n2, dtype=np.int32), diam_ft=diam, len_ft=length,
+        roughness=c, km_int=np.zeros(L), r_hw=r,
+        init_status=np.asarray(status, dtype=np.int8), valve_setting_user=setting,
+        dem_node=junc2.astype(np.int32), dem_base_cfs=d0[junc2],
+        dem_pat=np.full(junc2.size, -1, dtype=np.int32),
+        pattern_ids=[], patterns=[], meta=_meta(duration_sec=0),
+        tank_node=tanks, tank_h0=h0, tank_hmin=hmin, tank_hmax=hmax, tank_area=area,
+        tank_vmin=np.zeros(n_tanks), tank_v0=(h0 - hmin) * area,
+        tank_vmax=(hmax - hmin) * area, tank_overflow=np.zeros(n_tanks, dtype=np.int8),
+        pump_link=np.asarray(pumps, dtype=np.int32),
+        pump_ptype=np.ones(n_pumps, dtype=np.int8), pump_h0=-a_ft, pump_r=pr,
+        pump_n=np.full(n_pumps, nexp), pump_q0=np.full(n_pumps, q_design),
+        pump_qmax=np.full(n_pumps, 1e10), pump_hmax=a_ft,
+        pump_upat=np.full(n_pumps, -1, dtype=np.int32),
+        pump_curve_q=np.zeros(0), pump_curve_h=np.zeros(0),
+        pump_curve_ptr=np.zeros(n_pumps + 1, dtype=np.int32))
+
+
+def diurnal(t_hours):
+    """Smooth 24-h demand multiplier in [0.5, 1.6], lowest at 00:00."""
+    return 1.05 - 0.55 * np.cos(2.0 * np.pi * np.asarray(t_hours, dtype=np.float64) / 24.0)
+
+
+def eps_demands(net, T, B, seed=0, sigma=0.15, t0_hours=0.0):
+    """Demands [T,B,N] (cfs): base * diurnal(t) * lognormal(0, sigma) noise
+    drawn per step, scenario and node."""
+    rng = np.random.default_rng(seed)
+    d0 = net.demand_cfs_at(0)
+    m = diurnal(t0_hours + np.arange(T))
+    noise = rng.lognormal(0.0, sigma, size=(T, B, net.N))
+    return d0[None, None, :] * m[:, None, None] * noise
+
+
+def config5_network(seed=5, tank_center_ft=None):
+    """Extended-period workload shape: about 20 000 junctions and 23 000
+    pipes, 4 power-function pumps (shutoff 40-60 m, exponent 1.85),
+    3 cylindrical tanks (15-30 m diameter, starting at mid-range) and
+    1 reservoir."""
+    return eps_network(seed, n_junc=20000, n_pipes=23000, n_pumps=4, n_tanks=3,
+                       tank_center_ft=tank_center_ft, base_lps=(0.02, 0.08),
+                       spacing_m=120.0)
