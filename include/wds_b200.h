@@ -110,7 +110,16 @@ typedef struct WdsNetwork {
   int32_t checkfreq, maxcheck, extra_iter;
   const int32_t* perm;           /* [Nj] elimination order of junction rows, or NULL */
   int32_t emitter_capacity;      /* emitters per scenario kept on chip (0: 64) */
+  int32_t layout;                /* WDS_LAYOUT_*: where the schedule tables and the
+                                    per-scenario state live (no counterpart in the
+                                    reference, which holds everything in torch tensors) */
 } WdsNetwork;
+
+/* WdsNetwork.layout */
+#define WDS_LAYOUT_AUTO   0      /* shared memory when it fits, else global             */
+#define WDS_LAYOUT_SHARED 1      /* 16-bit tables and state in shared memory, or fail   */
+#define WDS_LAYOUT_GLOBAL 2      /* 32-bit tables and state in global memory, one CTA
+                                    per scenario (large networks)                         */
 
 /* Options of one forward call. */
 typedef struct WdsForwardOpts {

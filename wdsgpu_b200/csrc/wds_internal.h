@@ -98,6 +98,10 @@ struct DevNet {
   // dense top block: levels [L0, nlev) = columns [cT, Nj), nT = Nj - cT
   // (nT = 0 and L0 = nlev when the network has none)
   int L0, cT, nT;
+  // large network: slot-valued tables are 32-bit and stay in global memory
+  // with the scenario state (one 256-thread CTA per scenario); otherwise the
+  // 16-bit tables are staged into shared memory
+  int wide;
   int emcap;  // emitters per scenario held in shared memory
 };
 
@@ -113,6 +117,7 @@ struct DevWork {
   double* scr;    // [B][nscr][Nj] scratch vectors
   double* lk;     // [B][2][L] link flows q and Y of the forward
   double* M;      // [B][nT][nT] inverse of the top block's Schur complement
+  unsigned char* state;  // [B][state bytes] scenario state of large networks (else null)
   int nscr;
   int* valid;     // [B] 1 when the terminal state is stored
 };

@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <string>
+#include <type_traits>
 
 #include "wds_internal.h"
 
@@ -46,15 +47,21 @@ struct Sh {
   int8_t* S;
 };
 
-// Shared-memory view of the compact tables (16-bit indices).
-struct STab {
-  const uint32_t* spair;      // [nnzL] update list: begin | count << 16 | diagonal << 31
-  const uint16_t* fpair;      // [3 * npairs] {slot L_ik, slot L_jk, slot 1/D_k}
-  const uint16_t* colptr;     // [Nj+1]
+// View of the compact schedule tables.  Slot-valued tables (positions in the
+// factor W, in the update-term list and in the row lists) hold Slot: uint16_t
+// for networks whose tables fit 16 bits (staged into shared memory), uint32_t
+// for large networks (tables read from global memory).  Junction, link and
+// incidence indices are 16-bit in both.
+template <class Slot>
+struct TabT {
+  static constexpr bool kWide = sizeof(Slot) == 4;
+  const uint32_t* spair;      // per slot: begin | count << 16 | diagonal << 31 (wide: 2 words, begin and count | diagonal << 31)
+  const Slot* fpair;          // [3 * terms] {slot L_ik, slot L_jk, slot 1/D_k}
+  const Slot* colptr;         // [Nj+1]
   const uint16_t* rowidx;     // [nnzL]
   const uint16_t* levptr;     // [nlev+1] columns of a level (columns numbered in level order)
-  const uint16_t* rptr;       // [Nj+1] row lists
-  const uint32_t* rent;       // row entries slot | k << 16
+  const Slot* rptr;           // [Nj+1] row lists
+  const uint32_t* rent;       // row entries slot | k << 16 (wide: 2 words, slot and k)
   const uint8_t* mfac;        // [nlev] mode: log2 G | wide << 7
   const uint8_t* mfwd;
   const uint8_t* mbwd;
@@ -65,19 +72,52 @@ struct STab {
   const int16_t* e2;
   const uint16_t* pptr;       // [npairs+1]
   const uint16_t* plink;      // link | PRV << 15
-  const uint16_t* pslot;      // [npairs]
-  const uint16_t* fill;       // [nfill]
-  const uint16_t* dslot;      // [nT (nT+1) / 2] slot of top-block entry (i >= j) or 0xffff
-};
+  const Slot* pslot;          // [npairs]
+  const Slot* fill;           // [nfill]
+  const Slot* dslot;          // [nT (nT+1) / 2] slot of top-block entry (i >= j) or all ones
 
-__device__ STab stab_view(const DevNet& n, const unsigned char* b) {
-  STab t;
+  // update list of the entry in `slot`: first term, term count, diagonal flag
+  __device__ __forceinline__ void sp(int slot, int& pb, int& cnt, bool& diag) const {
+    if constexpr (kWide) {
+      const uint2 w = reinterpret_cast<const uint2*>(spair)[slot];
+      pb = (int)w.x;
+      cnt = (int)(w.y & 0x7fffffffu);
+      diag = (w.y >> 31) != 0;
+    } else {
+      const uint32_t w = spair[slot];
+      pb = (int)(w & 0xffffu);
+      cnt = (int)((w >> 16) & 0x7fffu);
+      diag = (w >> 31) != 0;
+    }
+  }
+  // row-list entry e: slot of L_jk and column k
+  __device__ __forceinline__ void re(int e, int& slot, int& k) const {
+    if constexpr (kWide) {
+      const uint2 w = reinterpret_cast<const uint2*>(rent)[e];
+      slot = (int)w.x;
+      k = (int)w.y;
+    } else {
+      const uint32_t w = rent[e];
+      slot = (int)(w & 0xffffu);
+      k = (int)(w >> 16);
+    }
+  }
+  __device__ __forceinline__ int cp(int j) const { return (int)colptr[j]; }
+};
+using STab = TabT<uint16_t>;
+using LTab = TabT<uint32_t>;
+
+template <class TB>
+__device__ TB tab_view(const DevNet& n, const unsigned char* b) {
+  using Slot = typename std::remove_pointer<decltype(TB::colptr)>::type;
+  using S = typename std::remove_const<Slot>::type;
+  TB t;
   t.spair = (const uint32_t*)(b + n.o_spair);
-  t.fpair = (const uint16_t*)(b + n.o_fpair);
-  t.colptr = (const uint16_t*)(b + n.o_colptr);
+  t.fpair = (const S*)(b + n.o_fpair);
+  t.colptr = (const S*)(b + n.o_colptr);
   t.rowidx = (const uint16_t*)(b + n.o_rowidx);
   t.levptr = (const uint16_t*)(b + n.o_levptr);
-  t.rptr = (const uint16_t*)(b + n.o_rptr);
+  t.rptr = (const S*)(b + n.o_rptr);
   t.rent = (const uint32_t*)(b + n.o_rent);
   t.mfac = (const uint8_t*)(b + n.o_mode);
   t.mfwd = t.mfac + n.nlev;
@@ -89,14 +129,15 @@ __device__ STab stab_view(const DevNet& n, const unsigned char* b) {
   t.e2 = (const int16_t*)(b + n.o_e2);
   t.pptr = (const uint16_t*)(b + n.o_pptr);
   t.plink = (const uint16_t*)(b + n.o_plink);
-  t.pslot = (const uint16_t*)(b + n.o_pslot);
-  t.fill = (const uint16_t*)(b + n.o_fill);
-  t.dslot = (const uint16_t*)(b + n.o_dslot);
+  t.pslot = (const S*)(b + n.o_pslot);
+  t.fill = (const S*)(b + n.o_fill);
+  t.dslot = (const S*)(b + n.o_dslot);
   return t;
 }
 
 // link index of an incidence entry (the upper bits carry flags)
-__device__ __forceinline__ int inc_link(const STab& T, int e) { return (int)(T.inc[e] & 0xffffu); }
+template <class TB>
+__device__ __forceinline__ int inc_link(const TB& T, int e) { return (int)(T.inc[e] & 0xffffu); }
 
 __device__ __forceinline__ double head_of(int c, const double* x, const double* hf) {
   return c >= 0 ? x[c] : hf[-c - 1];
@@ -301,7 +342,8 @@ __device__ __forceinline__ void link_coef(const DevNet& n, int k, double q, int 
 // Matrix-free (A x)_p of the node matrix: links with conductance P, emitter
 // diagonal emh, CBIG on the downstream node of ACTIVE PRVs
 // (dgga/autodiff.py:878-895; the same operator the forward assembles).
-__device__ __forceinline__ double amul_node(const DevNet& n, const STab& T, const Sh& s, int p,
+template <class TB>
+__device__ __forceinline__ double amul_node(const DevNet& n, const TB& T, const Sh& s, int p,
                                             const double* x) {
   const double* P = s.P;
   const int8_t* S = s.S;
@@ -336,26 +378,28 @@ __device__ __forceinline__ double group_sum(double v, int lg) {
 // block) on `nthr` threads (thread index t): the entries are split over lane
 // groups of 1 << lg, each group reducing its entry's update list with warp
 // shuffles.  Diagonal entries of factored columns become 1/D.
-__device__ __forceinline__ void fac_range(const STab& T, double* W, int t0, int t1, int lg, int t,
+template <class TB>
+__device__ __forceinline__ void fac_range(const TB& T, double* W, int t0, int t1, int lg, int t,
                                           int nthr, bool& bad) {
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = t0; base < t1; base += per) {
     const int slot = base + (t >> lg);
     const bool valid = slot < t1;
-    uint32_t sp = 0;
+    bool diag = false;
     double acc = 0.0;
     if (valid) {
-      sp = T.spair[slot];
-      const int pb = sp & 0xffff, pe = pb + (int)((sp >> 16) & 0x7fff);
+      int pb, cnt;
+      T.sp(slot, pb, cnt, diag);
+      const int pe = pb + cnt;
       for (int pr = pb + li; pr < pe; pr += G) {
-        const uint16_t* f = T.fpair + 3 * pr;
+        const auto* f = T.fpair + 3 * pr;
         acc += W[f[0]] * W[f[1]] * W[f[2]];
       }
     }
     acc = group_sum(acc, lg);
     if (valid && li == 0) {
       const double w = W[slot] - acc;
-      if (sp >> 31) {
+      if (diag) {
         if (!(w > 0.0) || !isfinite(w)) bad = true;
         W[slot] = 1.0 / w;
       } else {
@@ -367,7 +411,8 @@ __device__ __forceinline__ void fac_range(const STab& T, double* W, int t0, int 
 
 // Forward substitution over rows [c0, c1): v_j = (v_j - sum_k L_jk D_k u_k) / D_j,
 // or, for the rows of the top block (top), v_j = v_j - sum over the lower columns.
-__device__ __forceinline__ void fwd_range(const STab& T, const double* W, double* v, int c0,
+template <class TB>
+__device__ __forceinline__ void fwd_range(const TB& T, const double* W, double* v, int c0,
                                           int c1, int lg, int t, int nthr, bool top) {
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
@@ -375,10 +420,11 @@ __device__ __forceinline__ void fwd_range(const STab& T, const double* W, double
     const bool valid = j < c1;
     double acc = 0.0;
     if (valid) {
-      const int e1 = T.rptr[j + 1];
-      for (int e = T.rptr[j] + li; e < e1; e += G) {
-        const uint32_t r = T.rent[e];
-        acc += W[r & 0xffff] * v[r >> 16];
+      const int e1 = (int)T.rptr[j + 1];
+      for (int e = (int)T.rptr[j] + li; e < e1; e += G) {
+        int sl, k;
+        T.re(e, sl, k);
+        acc += W[sl] * v[k];
       }
     }
     acc = group_sum(acc, lg);
@@ -387,7 +433,8 @@ __device__ __forceinline__ void fwd_range(const STab& T, const double* W, double
 }
 
 // One backward-substitution level: x_j = u_j - (1/D_j) sum_i L_ij D_j x_i.
-__device__ __forceinline__ void bwd_level(const STab& T, const double* W, double* v, int lv,
+template <class TB>
+__device__ __forceinline__ void bwd_level(const TB& T, const double* W, double* v, int lv,
                                           int lg, int t, int nthr) {
   const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
@@ -422,8 +469,8 @@ __device__ __forceinline__ void bwd_level(const STab& T, const double* W, double
 // written to Mg (row-major, both triangles).  Returns 1 when this thread
 // owned a pivot that was not positive and finite.  Runs as a separate
 // function so that its block of registers does not add to the caller's.
-template <int NT>
-__device__ __noinline__ int top_inverse(const double* W, const uint16_t* dslot, double* tb,
+template <int NT, class Slot>
+__device__ __noinline__ int top_inverse(const double* W, const Slot* dslot, double* tb,
                                         double* Mg, int nT) {
   static_assert(NT == 256 && WDS_TOP_MAX == 48, "16 x 16 threads x 3 x 3 entries");
   constexpr int ST = WDS_TOP_MAX + 1;
@@ -437,8 +484,8 @@ __device__ __noinline__ int top_inverse(const double* W, const uint16_t* dslot, 
       const int i = r + 16 * ia, j = c + 16 * ib;
       double x = 0.0;
       if (i < nT && j <= i) {
-        const int sl = dslot[i * (i + 1) / 2 + j];
-        if (sl != 0xffff) x = W[sl];
+        const Slot sl = dslot[i * (i + 1) / 2 + j];
+        if (sl != (Slot)~Slot(0)) x = W[sl];
       }
       a[ia][ib] = x;
     }
@@ -551,8 +598,8 @@ __device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
 // the columns below the top block; the top block's slots hold its Schur
 // complement and its inverse goes to s.Mg.  Returns true when every pivot was
 // positive and finite.
-template <int NT>
-__device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
+template <int NT, class TB>
+__device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
   bool bad = false, prev_wide = true;
@@ -585,8 +632,8 @@ __device__ bool factor(const DevNet& n, const STab& T, const Sh& s) {
 
 // In-place (L D L^T) v = b: forward levels below the top block, the top rows'
 // right-hand side, the dense top solve, backward levels below the top block.
-template <int NT>
-__device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
+template <int NT, class TB>
+__device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
   bool prev_wide = true;
@@ -631,8 +678,8 @@ __device__ void solve(const DevNet& n, const STab& T, const Sh& s, double* v) {
 
 // x = A^{-1} rhs with `refine` refinement steps against the matrix-free A.
 // unit >= 0 means rhs = e_unit.
-template <int NT>
-__device__ void solve_refined(const DevNet& n, const STab& T, const Sh& s, const double* rhs,
+template <int NT, class TB>
+__device__ void solve_refined(const DevNet& n, const TB& T, const Sh& s, const double* rhs,
                               int unit, double* x, double* t, int refine) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) x[p] = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
@@ -682,8 +729,8 @@ __device__ void dense_solve(double* C, double* y, int m) {
 // ---------------------------------------------------------------- assembly
 // GGA assembly (linkcoeffs -> emittercoeffs -> nodecoeffs, solver.py:2958-3007)
 // into W (pattern of L) and F = V0; Xflow saved for PRV downstream nodes.
-template <int NT>
-__device__ void assemble_gga(const DevNet& n, const STab& T, const Sh& s, const double* kerow,
+template <int NT, class TB>
+__device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const double* kerow,
                              const double* drow) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) {
@@ -772,8 +819,8 @@ __device__ void assemble_gga(const DevNet& n, const STab& T, const Sh& s, const 
 
 // Reduced-matrix assembly at the current state (dgga/autodiff.py:928-962):
 // every link with its P, + emh diagonal, + CBIG on ACTIVE PRV downstream nodes.
-template <int NT>
-__device__ void assemble_reduced(const DevNet& n, const STab& T, const Sh& s) {
+template <int NT, class TB>
+__device__ void assemble_reduced(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) {
     double dg = 0.0;
@@ -822,8 +869,8 @@ __device__ void adj_coeffs(const DevNet& n, const Sh& s, const double* rrow,
 // true M_p.  The Woodbury columns A^{-1} e_u come from one substitution each;
 // the outer refinement makes the result independent of their rounding.
 // rhs: V0 (kept), result in dH.
-template <int NT>
-__device__ void primal_solve(const DevNet& n, const STab& T, const Sh& s, double* rp, double* dH,
+template <int NT, class TB>
+__device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
                              bool any_act, int refine) {
   const double* rhs = s.V0;
@@ -1008,20 +1055,29 @@ __device__ bool build_emitters(const DevNet& n, const Sh& s, const double* val, 
 }
 
 // ---------------------------------------------------------------- forward kernel
-template <int NT, int GR>
+template <int NT, int GR, class TB>
 __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
                                                         int state_bytes) {
   const int groups = GR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // stage the schedule tables once per CTA
-  for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
-    ((uint4*)smem_raw)[i] = n.stab[i];
-  __syncthreads();
-  const STab T = stab_view(n, smem_raw);
   const int g = threadIdx.x / NT;
   const int b = blockIdx.x * groups + g;
-  if (b >= a.B) return;  // a whole group; other groups use their own barrier
-  Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  TB T;
+  Sh s;
+  if constexpr (TB::kWide) {
+    // large network: tables and scenario state stay in global memory
+    if (b >= a.B) return;
+    T = tab_view<TB>(n, (const unsigned char*)n.stab);
+    s = carve(n, w.state + (size_t)b * state_bytes);
+  } else {
+    // stage the schedule tables once per CTA
+    for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
+      ((uint4*)smem_raw)[i] = n.stab[i];
+    __syncthreads();
+    T = tab_view<TB>(n, smem_raw);
+    if (b >= a.B) return;  // a whole group; other groups use their own barrier
+    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  }
   s.q = w.lk + (size_t)b * 2 * n.L;
   s.Y = s.q + n.L;
   s.Mg = w.M + (size_t)b * n.nT * n.nT;
@@ -1324,19 +1380,27 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
 // ---------------------------------------------------------------- adjoint kernel
 // Node adjoint with constraint rows (autodiff.py:1107-1154) and the
 // theta contraction (autodiff.py:1246-1312).
-template <int NT, int GR>
+template <int NT, int GR, class TB>
 __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
                                                         int state_bytes) {
   const int groups = GR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
-    ((uint4*)smem_raw)[i] = n.stab[i];
-  __syncthreads();
-  const STab T = stab_view(n, smem_raw);
   const int g = threadIdx.x / NT;
   const int b = blockIdx.x * groups + g;
-  if (b >= a.B) return;
-  Sh s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  TB T;
+  Sh s;
+  if constexpr (TB::kWide) {
+    if (b >= a.B) return;
+    T = tab_view<TB>(n, (const unsigned char*)n.stab);
+    s = carve(n, w.state + (size_t)b * state_bytes);
+  } else {
+    for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
+      ((uint4*)smem_raw)[i] = n.stab[i];
+    __syncthreads();
+    T = tab_view<TB>(n, smem_raw);
+    if (b >= a.B) return;
+    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  }
   s.Mg = w.M + (size_t)b * n.nT * n.nT;  // terminal top-block inverse of the forward
   if (!w.valid[b]) return;  // uniform per group
   const double* Wt = w.W + (size_t)b * n.nnzL;
@@ -1501,10 +1565,11 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int grou
     return WDS_E_UNSUPPORTED;
   }
   const int st = (int)smem_bytes(n);
-  const size_t smem = (size_t)n.stab_bytes + (size_t)groups * st;
+  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
   void (*kern)(DevNet, DevWork, FwdArgs, int) =
-      groups == 1 ? k_forward<256, 1> : groups == 2 ? k_forward<256, 2> : groups == 3 ? k_forward<256, 3>
-                                                                             : k_forward<256, 4>;
+      n.wide ? k_forward<256, 1, LTab>
+      : groups == 1 ? k_forward<256, 1, STab> : groups == 2 ? k_forward<256, 2, STab>
+      : groups == 3 ? k_forward<256, 3, STab> : k_forward<256, 4, STab>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward: ") + cudaGetErrorString(ce);
@@ -1527,10 +1592,11 @@ int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int grou
     return WDS_E_UNSUPPORTED;
   }
   const int st = (int)smem_bytes(n);
-  const size_t smem = (size_t)n.stab_bytes + (size_t)groups * st;
+  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
   void (*kern)(DevNet, DevWork, AdjArgs, int) =
-      groups == 1 ? k_adjoint<256, 1> : groups == 2 ? k_adjoint<256, 2> : groups == 3 ? k_adjoint<256, 3>
-                                                                             : k_adjoint<256, 4>;
+      n.wide ? k_adjoint<256, 1, LTab>
+      : groups == 1 ? k_adjoint<256, 1, STab> : groups == 2 ? k_adjoint<256, 2, STab>
+      : groups == 3 ? k_adjoint<256, 3, STab> : k_adjoint<256, 4, STab>;
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_adjoint: ") + cudaGetErrorString(ce);

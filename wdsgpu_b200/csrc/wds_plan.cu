@@ -311,13 +311,10 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     md_bwd[l] = pick_mode(levptr[l1] - levptr[l], mc);
     if (l1 == nlev) break;
   }
-  // dense position (i, j), i >= j, of the top block -> slot of L, or 0xffff
-  std::vector<uint16_t> s_ds((size_t)std::max(nT * (nT + 1) / 2, 1), (uint16_t)0xffff);
+  // dense position (i, j), i >= j, of the top block -> slot of L, or -1
+  std::vector<int> dsl((size_t)std::max(nT * (nT + 1) / 2, 1), -1);
   for (int i = 0; i < nT; ++i)
-    for (int j = 0; j <= i; ++j) {
-      const int sl = slot(cT + i, cT + j);
-      if (sl >= 0) s_ds[(size_t)i * (i + 1) / 2 + j] = (uint16_t)sl;
-    }
+    for (int j = 0; j <= i; ++j) dsl[(size_t)i * (i + 1) / 2 + j] = slot(cT + i, cT + j);
   // ---- link end codes, incidence lists, pairs
   auto code = [&](int nd) { return jrow[nd] >= 0 ? iperm[jrow[nd]] : -(fix_idx[nd] + 1); };
   std::vector<int> e1(L), e2(L);
@@ -448,7 +445,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       ok = ok && in(fitem[t].x, 0, Nj) && fitem[t].y >= 0 && fitem[t].y <= fitem[t].z &&
            fitem[t].z <= (int)rent.size() && in(fitem[t].w, 0, nnzL) && in(bitem[t].x, 0, Nj) &&
            bitem[t].y >= 0 && bitem[t].y < bitem[t].z && bitem[t].z <= nnzL;
-    for (uint16_t v : s_ds) ok = ok && (v == 0xffff || in(v, colptr[cT], nnzL));
+    for (int v : dsl) ok = ok && (v == -1 || in(v, colptr[cT], nnzL));
     ok = ok && nT >= 0 && nT <= WDS_TOP_MAX;
     for (int v : cb_idx) ok = ok && in(v, 0, std::max(npcv, 1));
     for (int i = 0; i < npcv; ++i)
@@ -465,32 +462,24 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int f = 0; f < Nf; ++f) ok = ok && in(fnodes[f], 0, N);
     if (!ok) return fail(WDS_E_ARG, "wds_plan: internal table failed its bounds check");
   }
-  // ---- compact tables (16-bit indices) staged in shared memory once per CTA
-  if (nnzL >= 65536 || Nj >= 32768 || Nf >= 16384 || L >= 32768 ||
-      (int)fpair.size() / 3 >= 65536 || (int)rent.size() >= 65536 || (int)inc.size() >= 65536 ||
-      (int)pair_link.size() >= 65536 || N >= 65536 || (int)ftask.size() >= 65536)
-    return fail(WDS_E_UNSUPPORTED, "wds_plan: network too large for the shared-memory schedule");
+  // ---- compact tables.  Junction, link and incidence indices are 16-bit.
+  // Slot-valued tables (positions in W, in the update-term list, in the row
+  // lists) are 16-bit and staged in shared memory when the network allows it
+  // (narrow layout); otherwise they are 32-bit and read from global memory,
+  // with the scenario state there too (wide layout, large networks).
+  if (Nj >= 32768 || Nf >= 16384 || L >= 32768 || N >= 65536 || (int)inc.size() >= 65536 ||
+      (int)pair_link.size() >= 65536)
+    return fail(WDS_E_UNSUPPORTED, "wds_plan: network too large (at most 32767 junctions and "
+                                   "32767 links)");
+  for (auto& t : ftask)
+    if (t.z - t.y >= 32768) return fail(WDS_E_UNSUPPORTED, "wds_plan: update list too long");
   // Columns are numbered in level order, so level l owns the columns
   // [levptr[l], levptr[l+1]) and the slots [colptr[levptr[l]], colptr[levptr[l+1]]).
-  // update list of every entry of L, by slot: begin | count << 16 | diagonal << 31
-  std::vector<uint32_t> s_sp(nnzL, 0);
-  for (auto& t : ftask) {
-    if (t.z - t.y >= 32768) return fail(WDS_E_UNSUPPORTED, "wds_plan: update list too long");
-    s_sp[t.x] = (uint32_t)t.y | ((uint32_t)(t.z - t.y) << 16) | ((uint32_t)t.w << 31);
-  }
-  std::vector<uint16_t> s_fp(fpair.begin(), fpair.end());
-  if (s_fp.empty()) s_fp.push_back(0);
-  std::vector<uint16_t> s_cp(colptr.begin(), colptr.end()), s_ri(rowidx.begin(), rowidx.end());
-  std::vector<uint16_t> s_lp(levptr.begin(), levptr.end());
-  // row lists (forward substitution): entries {slot of L_jk | k << 16} of row j
-  // at [rptr[j], rptr[j+1])
-  std::vector<uint16_t> s_rp(Nj + 1, 0);
-  for (int j = 0; j < Nj; ++j) s_rp[j + 1] = (uint16_t)fitem[j].z;
   for (int j = 0; j < Nj; ++j)
-    if (fitem[j].x != j || fitem[j].y != s_rp[j])
+    if (fitem[j].x != j || (j > 0 && fitem[j].y != fitem[j - 1].z) || (j == 0 && fitem[0].y != 0))
       return fail(WDS_E_ARG, "wds_plan: internal error (row list order)");
-  std::vector<uint32_t> s_re(rent.size());
-  for (size_t e = 0; e < rent.size(); ++e) s_re[e] = (uint32_t)rent[e].x | ((uint32_t)rent[e].y << 16);
+  std::vector<uint16_t> s_ri(rowidx.begin(), rowidx.end());
+  std::vector<uint16_t> s_lp(levptr.begin(), levptr.end());
   std::vector<uint8_t> s_md;
   s_md.insert(s_md.end(), md_fac.begin(), md_fac.end());
   s_md.insert(s_md.end(), md_fwd.begin(), md_fwd.end());
@@ -509,27 +498,77 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     }
   if (s_in.empty()) s_in.push_back(0);
   std::vector<int16_t> s_e1(e1.begin(), e1.end()), s_e2(e2.begin(), e2.end());
-  std::vector<uint16_t> s_pp(pair_ptr.begin(), pair_ptr.end()), s_ps(pair_slot.begin(), pair_slot.end());
+  std::vector<uint16_t> s_pp(pair_ptr.begin(), pair_ptr.end());
   std::vector<uint16_t> s_pl(pair_link.size());
   for (size_t e = 0; e < pair_link.size(); ++e)
     s_pl[e] = (uint16_t)(pair_link[e] | (net->link_kind[pair_link[e]] == WDS_KIND_PRV ? 0x8000 : 0));
   if (s_pl.empty()) s_pl.push_back(0);
-  if (s_ps.empty()) s_ps.push_back(0);
-  std::vector<uint16_t> s_fl(fill_slot.begin(), fill_slot.end());
-  if (s_fl.empty()) s_fl.push_back(0);
-  Blob sblob;
-  auto sadd = [&](auto& v) {
-    size_t off = (sblob.bytes.size() + 15) / 16 * 16;
-    size_t nb = v.size() * sizeof(v[0]);
-    sblob.bytes.resize(off + nb);
-    if (nb) std::memcpy(sblob.bytes.data() + off, v.data(), nb);
-    return (int)off;
+  struct TabOff { int sp, fp, cp, ri, lp, rp, re, md, ip, is, in, e1, e2, pp, pl, ps, fl, ds; };
+  auto pack = [&](auto tag, Blob& sb, TabOff& o) {
+    using S = decltype(tag);
+    constexpr bool W32 = sizeof(S) == 4;
+    auto sadd = [&](auto& v) {
+      size_t off = (sb.bytes.size() + 15) / 16 * 16;
+      size_t nb = v.size() * sizeof(v[0]);
+      sb.bytes.resize(off + nb);
+      if (nb) std::memcpy(sb.bytes.data() + off, v.data(), nb);
+      return (int)off;
+    };
+    // update list of every entry of L, by slot (narrow: begin | count << 16 |
+    // diagonal << 31; wide: begin, count | diagonal << 31)
+    std::vector<uint32_t> sp((size_t)nnzL * (W32 ? 2 : 1), 0);
+    for (auto& t : ftask) {
+      const uint32_t hi = (uint32_t)(t.z - t.y) | ((uint32_t)t.w << 31);
+      if (W32) { sp[2 * (size_t)t.x] = (uint32_t)t.y; sp[2 * (size_t)t.x + 1] = hi; }
+      else sp[t.x] = (uint32_t)t.y | ((uint32_t)(t.z - t.y) << 16) | ((uint32_t)t.w << 31);
+    }
+    std::vector<S> fp(fpair.begin(), fpair.end());
+    if (fp.empty()) fp.push_back(0);
+    std::vector<S> cp(colptr.begin(), colptr.end());
+    // row lists (forward substitution): entries {slot of L_jk, k} of row j at [rptr[j], rptr[j+1])
+    std::vector<S> rp(Nj + 1, 0);
+    for (int j = 0; j < Nj; ++j) rp[j + 1] = (S)fitem[j].z;
+    std::vector<uint32_t> re(rent.size() * (W32 ? 2 : 1));
+    for (size_t e = 0; e < rent.size(); ++e) {
+      if (W32) { re[2 * e] = (uint32_t)rent[e].x; re[2 * e + 1] = (uint32_t)rent[e].y; }
+      else re[e] = (uint32_t)rent[e].x | ((uint32_t)rent[e].y << 16);
+    }
+    std::vector<S> ps(pair_slot.begin(), pair_slot.end());
+    if (ps.empty()) ps.push_back(0);
+    std::vector<S> fl(fill_slot.begin(), fill_slot.end());
+    if (fl.empty()) fl.push_back(0);
+    std::vector<S> ds(dsl.size());
+    for (size_t i = 0; i < dsl.size(); ++i) ds[i] = dsl[i] < 0 ? (S)~S(0) : (S)dsl[i];
+    o.sp = sadd(sp); o.fp = sadd(fp); o.cp = sadd(cp); o.ri = sadd(s_ri); o.lp = sadd(s_lp);
+    o.rp = sadd(rp); o.re = sadd(re); o.md = sadd(s_md); o.ip = sadd(s_ip); o.is = sadd(s_is);
+    o.in = sadd(s_in); o.e1 = sadd(s_e1); o.e2 = sadd(s_e2); o.pp = sadd(s_pp); o.pl = sadd(s_pl);
+    o.ps = sadd(ps); o.fl = sadd(fl); o.ds = sadd(ds);
+    sb.bytes.resize((sb.bytes.size() + 15) / 16 * 16);
   };
-  const int so_sp = sadd(s_sp), so_fp = sadd(s_fp), so_cp = sadd(s_cp),
-            so_ri = sadd(s_ri), so_lp = sadd(s_lp), so_rp = sadd(s_rp), so_re = sadd(s_re), so_md = sadd(s_md), so_ip = sadd(s_ip), so_is = sadd(s_is),
-            so_in = sadd(s_in), so_e1 = sadd(s_e1), so_e2 = sadd(s_e2), so_pp = sadd(s_pp),
-            so_pl = sadd(s_pl), so_ps = sadd(s_ps), so_fl = sadd(s_fl), so_ds = sadd(s_ds);
-  sblob.bytes.resize((sblob.bytes.size() + 15) / 16 * 16);
+  const bool fits16 = nnzL < 65535 && (int)fpair.size() / 3 < 65536 &&
+                      (int)rent.size() < 65536 && (int)fitem.back().z < 65536;
+  // per-scenario state of the shared-memory layout (sizes only)
+  DevNet dsz{};
+  dsz.N = N; dsz.L = L; dsz.Nj = Nj; dsz.Nf = Nf; dsz.nnzL = nnzL; dsz.npcv = npcv;
+  dsz.nxf = nxf; dsz.nT = nT;
+  dsz.emcap = std::min(Nj, net->emitter_capacity > 0 ? net->emitter_capacity : 64);
+  const size_t state_bytes = state_smem_bytes(dsz);
+  Blob sblob;
+  TabOff to{};
+  if (net->layout < WDS_LAYOUT_AUTO || net->layout > WDS_LAYOUT_GLOBAL)
+    return fail(WDS_E_ARG, "wds_plan: unknown layout");
+  bool wide = !fits16 || net->layout == WDS_LAYOUT_GLOBAL;
+  if (!wide) {
+    pack(uint16_t{}, sblob, to);
+    wide = sblob.bytes.size() + state_bytes > 227 * 1024;
+  }
+  if (wide && net->layout == WDS_LAYOUT_SHARED)
+    return fail(WDS_E_UNSUPPORTED, "wds_plan: the network's tables and state exceed shared "
+                                   "memory (layout WDS_LAYOUT_SHARED)");
+  if (wide) {
+    sblob = Blob();
+    pack(uint32_t{}, sblob, to);
+  }
   std::vector<unsigned char> stab_bytes = sblob.bytes;
   // ---- upload
   Blob blob;
@@ -591,12 +630,13 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.tl_other = P_(int, o_tlo); d.tl_qsign = P_(double, o_tlq); d.tl_hmax = P_(double, o_tlx);
   d.tl_hmin = P_(double, o_tln); d.tl_flags = P_(uint8_t, o_tlf);
   d.stab = P_(uint4, o_stab);
-  d.stab_bytes = (int)stab_bytes.size();
-  d.o_spair = so_sp; d.o_fpair = so_fp; d.o_colptr = so_cp;
-  d.o_rowidx = so_ri; d.o_levptr = so_lp; d.o_rptr = so_rp;
-  d.o_rent = so_re; d.o_mode = so_md; d.o_inc_ptr = so_ip; d.o_inc_split = so_is;
-  d.o_inc = so_in; d.o_e1 = so_e1; d.o_e2 = so_e2; d.o_pptr = so_pp; d.o_plink = so_pl;
-  d.o_pslot = so_ps; d.o_fill = so_fl; d.o_dslot = so_ds;
+  d.wide = wide ? 1 : 0;
+  d.stab_bytes = wide ? 0 : (int)stab_bytes.size();  // staged into shared memory (narrow only)
+  d.o_spair = to.sp; d.o_fpair = to.fp; d.o_colptr = to.cp;
+  d.o_rowidx = to.ri; d.o_levptr = to.lp; d.o_rptr = to.rp;
+  d.o_rent = to.re; d.o_mode = to.md; d.o_inc_ptr = to.ip; d.o_inc_split = to.is;
+  d.o_inc = to.in; d.o_e1 = to.e1; d.o_e2 = to.e2; d.o_pptr = to.pp; d.o_plink = to.pl;
+  d.o_pslot = to.ps; d.o_fill = to.fl; d.o_dslot = to.ds;
   d.L0 = L0; d.cT = cT; d.nT = nT;
 #undef P_
   d.hexp = net->hexp; d.qexp = net->qexp; d.rqtol = net->rqtol; d.htol = net->htol;
@@ -607,7 +647,10 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   plan->threads = 256;
   // scenario groups per CTA: the count that keeps the most scenarios resident
   // per SM (228 KB of shared memory per SM, 1 KB reserved per CTA)
-  {
+  if (d.wide) {  // large network: one 256-thread CTA per scenario, state in global memory
+    plan->groups = 1;
+    plan->smem_fwd = plan->smem_adj = 0;
+  } else {
     const size_t st = state_smem_bytes(d);
     int best_g = 0, best_res = 0;
     for (int g = 1; g <= 4; ++g) {
@@ -621,7 +664,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     plan->smem_fwd = best_g ? (size_t)d.stab_bytes + best_g * st : (size_t)d.stab_bytes + st;
     plan->smem_adj = plan->smem_fwd;
   }
-  if (plan->groups == 0 || plan->smem_fwd > 227 * 1024) {
+  if (plan->groups == 0 || (!d.wide && plan->smem_fwd > 227 * 1024)) {
     cudaFree(plan->dtab);
     delete plan;
     return fail(WDS_E_UNSUPPORTED,
@@ -638,7 +681,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   size_t ow = take(B * nnzL * 8), op = take(B * L * 8), odr = take(B * L * 8),
          oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
          oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4),
-         olk = take(B * 2 * L * 8), otop = take(B * std::max(nT * nT, 1) * 8);
+         olk = take(B * 2 * L * 8), otop = take(B * std::max(nT * nT, 1) * 8),
+         ostate = take(d.wide ? B * state_bytes : 0);
   if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
     cudaFree(plan->dtab);
     delete plan;
@@ -650,6 +694,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
   w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
+  w.state = d.wide ? wb + ostate : nullptr;
   // ---- host copy of the symbolic structure
   HostSym& hs = plan->sym;
   hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
@@ -797,7 +842,8 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   const size_t ow = take(B * d.nnzL * 8), op = take(B * d.L * 8), odr = take(B * d.L * 8),
                oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
                oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4),
-               olk = take(B * 2 * d.L * 8), otop = take(B * std::max(d.nT * d.nT, 1) * 8);
+               olk = take(B * 2 * d.L * 8), otop = take(B * std::max(d.nT * d.nT, 1) * 8),
+               ostate = take(d.wide ? B * state_smem_bytes(d) : 0);
   if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
     const size_t per = bytes / B;
     return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
@@ -815,6 +861,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
   w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
+  w.state = d.wide ? wb + ostate : nullptr;
   w.nscr = nscr;
   FwdArgs a{};
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;

@@ -73,6 +73,8 @@ class _Plan:
         net.extra_iter = solver.extra_iter
         net.perm = None if solver.perm is None else _ptr(solver.perm, ctypes.c_int32)
         net.emitter_capacity = int(solver.emitter_capacity)
+        net.layout = {"auto": _lib.LAYOUT_AUTO, "shared": _lib.LAYOUT_SHARED,
+                      "global": _lib.LAYOUT_GLOBAL}[solver.sm100_layout]
         with torch.cuda.device(self.device):
             _lib.check(lib.wds_plan(ctypes.byref(net), self.max_batch,
                                     ctypes.byref(self.handle)), "wds_plan")
@@ -135,6 +137,10 @@ class GGASolver:
 
     `sm100_refine` (default 2) is the number of iterative-refinement steps of
     every linear solve, mirroring `dense_refine` / `cudss_refine`.
+    `sm100_layout` ("auto", "shared" or "global", set before the first solve)
+    says where the schedule tables and per-scenario state live: shared memory
+    (several scenarios per SM), or global memory for networks too large for
+    it ("auto" picks shared memory when it fits).
     """
 
     def __init__(self, net, device="cuda", dtype=torch.float64, mode="dense",
@@ -156,6 +162,7 @@ class GGASolver:
         self.dtype = dtype
         self.net = net
         self.sm100_refine = 2
+        self.sm100_layout = "auto"
         # emitters per scenario kept in shared memory (junctions with Ke > 0)
         self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
         lt = np.asarray(net.link_type, dtype=np.int64)

@@ -537,3 +537,41 @@ def config5_network(seed=5, tank_center_ft=None):
     return eps_network(seed, n_junc=20000, n_pipes=23000, n_pumps=4, n_tanks=3,
                        tank_center_ft=tank_center_ft, base_lps=(0.02, 0.08),
                        spacing_m=120.0)
+
+
+def tcv_network(seed=3, n_junc=542, n_links=554, n_tcv=79, km_range=(1.0, 20.0)):
+    """Looped network whose `n_tcv` links are throttle control valves (Km in
+    `km_range`, fully open TCVs for a quarter of them: Km = 0)."""
+    base = looped_network(seed, n_junc=n_junc, n_res=2, n_pipes=n_links, spacing_m=160.0)
+    rng = np.random.default_rng(seed + 300)
+    L = base.L
+    res = set(np.flatnonzero(base.node_type == RESERVOIR).tolist())
+    cand = [k for k in range(L)
+            if base.link_n1[k] not in res and base.link_n2[k] not in res]
+    tcv = np.sort(rng.choice(cand, size=n_tcv, replace=False))
+    ltype = base.link_type.copy()
+    ltype[tcv] = TCV
+    status = base.init_status.copy()
+    status[tcv] = 2
+    setting = base.valve_setting_user.copy()
+    setting[tcv] = rng.uniform(*km_range, n_tcv)
+    setting[tcv[: n_tcv // 4]] = 0.0
+    c = base.roughness.copy()
+    length = base.len_ft.copy()
+    c[tcv] = 0.0
+    length[tcv] = 0.0
+    f = dict(base.as_fields())
+    f.update(link_type=ltype, init_status=status, valve_setting_user=setting, roughness=c,
+             len_ft=length, r_hw=_r_hw(length, c, base.diam_ft))
+    return Net(**f)
+
+
+def config3_networks(seed=3):
+    """The four networks of the mixed-size workload: 100 junctions / 120
+    pipes; 542 junctions / 554 links including 79 throttle control valves;
+    782 junctions / 905 pipes / 3 PRVs (the config-2 network); 3000 junctions
+    / 3600 pipes."""
+    return [looped_network(seed, n_junc=100, n_res=1, n_pipes=120),
+            tcv_network(seed + 1),
+            config2_network(),
+            looped_network(seed + 2, n_junc=3000, n_res=2, n_pipes=3600, spacing_m=150.0)]
