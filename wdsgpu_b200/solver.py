@@ -502,7 +502,9 @@ class GGASolver:
         o.r_stride = 0 if r.shape[0] == 1 else self.L
         for name, t, cols in (("q0", q0, self.L), ("e0", e0, self.N)):
             if t is not None:
-                if (t.dtype != torch.float64 or t.device != dev or not t.is_contiguous()
+                same_dev = t.device.type == dev.type and (dev.index is None
+                                                          or t.device.index == dev.index)
+                if (t.dtype != torch.float64 or not same_dev or not t.is_contiguous()
                         or tuple(t.shape) != (B, cols)):
                     raise ValueError("%s must be a contiguous float64 [%d, %d] tensor on %s"
                                      % (name, B, cols, dev))

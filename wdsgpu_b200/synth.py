@@ -575,3 +575,21 @@ def config3_networks(seed=3):
             tcv_network(seed + 1),
             config2_network(),
             looped_network(seed + 2, n_junc=3000, n_res=2, n_pipes=3600, spacing_m=150.0)]
+
+
+def tanks_as_junctions(net):
+    """The same network with every tank turned into a zero-demand junction
+    (for a steady pre-solve that finds the grade line at the tank sites)."""
+    f = dict(net.as_fields())
+    tn = np.asarray(net.tank_node if net.tank_node is not None else [], dtype=np.int64)
+    nt = np.asarray(f["node_type"]).copy()
+    nt[tn] = JUNCTION
+    junc = np.flatnonzero(nt == JUNCTION)
+    d0 = net.demand_cfs_at(0)
+    f.update(node_type=nt, dem_node=junc.astype(np.int32), dem_base_cfs=d0[junc],
+             dem_pat=np.full(junc.size, -1, np.int32), tank_node=np.zeros(0, np.int32),
+             tank_overflow=np.zeros(0, np.int8))
+    for k in ("tank_h0", "tank_hmin", "tank_hmax", "tank_area", "tank_vmin", "tank_v0",
+              "tank_vmax"):
+        f[k] = np.zeros(0)
+    return Net(**f)
