@@ -113,6 +113,10 @@ typedef struct WdsNetwork {
   int32_t layout;                /* WDS_LAYOUT_*: where the schedule tables and the
                                     per-scenario state live (no counterpart in the
                                     reference, which holds everything in torch tensors) */
+  int32_t factor_fp32;           /* 1: LDL^T factor and substitutions in FP32, every
+                                    solve refined against the FP64 operator (the
+                                    precision choice dense_refine / cudss_refine leave
+                                    open, dgga/solver.py:182, 384); 0: FP64 */
 } WdsNetwork;
 
 /* WdsNetwork.layout */

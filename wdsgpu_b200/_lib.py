@@ -50,7 +50,7 @@ class WdsNetwork(ctypes.Structure):
         ("extra_iter", ctypes.c_int32),
         ("perm", c_int32_p),
         ("emitter_capacity", ctypes.c_int32),
-        ("layout", ctypes.c_int32),
+        ("layout", ctypes.c_int32), ("factor_fp32", ctypes.c_int32),
     ]
 
 

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .solver import CBIG, GGASolver
+from .solver import CBIG, GGASolver, _not_pd_hint
 
 __all__ = ["implicit_solve", "ImplicitGGASolveSM100", "hw_resistance", "dr_dC"]
 
@@ -88,7 +88,7 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
             if np_:
                 raise RuntimeError(
                     "adjoint='gpu': the node matrix of scenarios %s is not positive "
-                    "definite" % np_[:8])
+                    "definite%s" % (np_[:8], _not_pd_hint(s)))
             raise RuntimeError(
                 "adjoint='gpu': scenarios %s did not converge (relerr=%s > accuracy=%g)"
                 % (bad[:8], [float(o["relerr"][b]) for b in bad[:4]], float(accuracy)))

@@ -102,12 +102,15 @@ struct DevNet {
   // with the scenario state (one 256-thread CTA per scenario); otherwise the
   // 16-bit tables are staged into shared memory
   int wide;
+  // factor and substitutions in FP32 (residuals, refinement and the Newton
+  // update stay in FP64)
+  int fp32;
   int emcap;  // emitters per scenario held in shared memory
 };
 
 // Workspace kept between the forward (implicit mode) and the adjoint.
 struct DevWork {
-  double* W;      // [B][nnzL] terminal factor (unscaled columns, 1/D on diagonal)
+  double* W;      // [B][nnzL] terminal factor (unscaled columns, 1/D on diagonal); float when fp32
   double* P;      // [B][L]
   double* dr;     // [B][L]
   double* emh;    // [B][Nj]

@@ -39,6 +39,7 @@ constexpr double kINF = __builtin_huge_val();
 
 struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
+  float* Wf;                      // the factor when it is kept in FP32 (W is then null)
   double *em_e, *em_ke, *em_emh;  // per emitter slot: flow, coefficient, 1/hgrad
   int16_t* eslot;                 // [Nj] emitter slot of a junction or -1
   double* tb;                     // [2][49] pivot columns (+ 1/pivot) of the top-block inversion
@@ -369,24 +370,34 @@ __device__ __forceinline__ double amul_node(const DevNet& n, const TB& T, const 
 
 // Sum over a lane group of size 1 << lg (aligned groups inside a warp); every
 // lane of the warp calls it with the same lg.
-__device__ __forceinline__ double group_sum(double v, int lg) {
+template <class FT>
+__device__ __forceinline__ FT group_sum(FT v, int lg) {
   for (int o = (1 << lg) >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// The factor of the scenario in its storage precision FT (double, or float
+// for the FP32 factor with FP64 refinement).
+template <class FT>
+__device__ __forceinline__ FT* wp(const Sh& s);
+template <>
+__device__ __forceinline__ double* wp<double>(const Sh& s) { return s.W; }
+template <>
+__device__ __forceinline__ float* wp<float>(const Sh& s) { return s.Wf; }
 
 // Factor slots [t0, t1) (one level, or the Schur-complement step of the top
 // block) on `nthr` threads (thread index t): the entries are split over lane
 // groups of 1 << lg, each group reducing its entry's update list with warp
 // shuffles.  Diagonal entries of factored columns become 1/D.
-template <class TB>
-__device__ __forceinline__ void fac_range(const TB& T, double* W, int t0, int t1, int lg, int t,
+template <class TB, class FT>
+__device__ __forceinline__ void fac_range(const TB& T, FT* W, int t0, int t1, int lg, int t,
                                           int nthr, bool& bad) {
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = t0; base < t1; base += per) {
     const int slot = base + (t >> lg);
     const bool valid = slot < t1;
     bool diag = false;
-    double acc = 0.0;
+    FT acc = 0;
     if (valid) {
       int pb, cnt;
       T.sp(slot, pb, cnt, diag);
@@ -398,10 +409,10 @@ __device__ __forceinline__ void fac_range(const TB& T, double* W, int t0, int t1
     }
     acc = group_sum(acc, lg);
     if (valid && li == 0) {
-      const double w = W[slot] - acc;
+      const FT w = W[slot] - acc;
       if (diag) {
-        if (!(w > 0.0) || !isfinite(w)) bad = true;
-        W[slot] = 1.0 / w;
+        if (!(w > FT(0)) || !isfinite(w)) bad = true;
+        W[slot] = FT(1) / w;
       } else {
         W[slot] = w;
       }
@@ -411,30 +422,33 @@ __device__ __forceinline__ void fac_range(const TB& T, double* W, int t0, int t1
 
 // Forward substitution over rows [c0, c1): v_j = (v_j - sum_k L_jk D_k u_k) / D_j,
 // or, for the rows of the top block (top), v_j = v_j - sum over the lower columns.
-template <class TB>
-__device__ __forceinline__ void fwd_range(const TB& T, const double* W, double* v, int c0,
+template <class TB, class FT>
+__device__ __forceinline__ void fwd_range(const TB& T, const FT* W, double* v, int c0,
                                           int c1, int lg, int t, int nthr, bool top) {
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
     const int j = base + (t >> lg);
     const bool valid = j < c1;
-    double acc = 0.0;
+    FT acc = 0;
     if (valid) {
       const int e1 = (int)T.rptr[j + 1];
       for (int e = (int)T.rptr[j] + li; e < e1; e += G) {
         int sl, k;
         T.re(e, sl, k);
-        acc += W[sl] * v[k];
+        acc += W[sl] * (FT)v[k];
       }
     }
     acc = group_sum(acc, lg);
-    if (valid && li == 0) v[j] = top ? v[j] - acc : (v[j] - acc) * W[T.colptr[j]];
+    if (valid && li == 0) {
+      const FT vj = (FT)v[j];
+      v[j] = (double)(top ? vj - acc : (vj - acc) * W[T.colptr[j]]);
+    }
   }
 }
 
 // One backward-substitution level: x_j = u_j - (1/D_j) sum_i L_ij D_j x_i.
-template <class TB>
-__device__ __forceinline__ void bwd_level(const TB& T, const double* W, double* v, int lv,
+template <class TB, class FT>
+__device__ __forceinline__ void bwd_level(const TB& T, const FT* W, double* v, int lv,
                                           int lg, int t, int nthr) {
   const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
@@ -442,14 +456,14 @@ __device__ __forceinline__ void bwd_level(const TB& T, const double* W, double* 
     const int j = base + (t >> lg);
     const bool valid = j < c1;
     int cb = 0;
-    double acc = 0.0;
+    FT acc = 0;
     if (valid) {
       cb = T.colptr[j];
       const int ce = T.colptr[j + 1];
-      for (int e = cb + 1 + li; e < ce; e += G) acc += W[e] * v[T.rowidx[e]];
+      for (int e = cb + 1 + li; e < ce; e += G) acc += W[e] * (FT)v[T.rowidx[e]];
     }
     acc = group_sum(acc, lg);
-    if (valid && li == 0) v[j] = v[j] - W[cb] * acc;
+    if (valid && li == 0) v[j] = (double)((FT)v[j] - W[cb] * acc);
   }
 }
 
@@ -469,8 +483,8 @@ __device__ __forceinline__ void bwd_level(const TB& T, const double* W, double* 
 // written to Mg (row-major, both triangles).  Returns 1 when this thread
 // owned a pivot that was not positive and finite.  Runs as a separate
 // function so that its block of registers does not add to the caller's.
-template <int NT, class Slot>
-__device__ __noinline__ int top_inverse(const double* W, const Slot* dslot, double* tb,
+template <int NT, class Slot, class FT>
+__device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* tb,
                                         double* Mg, int nT) {
   static_assert(NT == 256 && WDS_TOP_MAX == 48, "16 x 16 threads x 3 x 3 entries");
   constexpr int ST = WDS_TOP_MAX + 1;
@@ -485,7 +499,7 @@ __device__ __noinline__ int top_inverse(const double* W, const Slot* dslot, doub
       double x = 0.0;
       if (i < nT && j <= i) {
         const Slot sl = dslot[i * (i + 1) / 2 + j];
-        if (sl != (Slot)~Slot(0)) x = W[sl];
+        if (sl != (Slot)~Slot(0)) x = (double)W[sl];
       }
       a[ia][ib] = x;
     }
@@ -598,7 +612,7 @@ __device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
 // the columns below the top block; the top block's slots hold its Schur
 // complement and its inverse goes to s.Mg.  Returns true when every pivot was
 // positive and finite.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
@@ -609,10 +623,10 @@ __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
     const int t0 = T.colptr[T.levptr[lv]], t1 = T.colptr[T.levptr[lv + 1]];
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      fac_range(T, s.W, t0, t1, md & 7, tid, NT, bad);
+      fac_range(T, wp<FT>(s), t0, t1, md & 7, tid, NT, bad);
       gsync<NT>();
     } else if (inw) {
-      fac_range(T, s.W, t0, t1, md & 7, lane, 32, bad);
+      fac_range(T, wp<FT>(s), t0, t1, md & 7, lane, 32, bad);
       __syncwarp();
     }
     prev_wide = wide;
@@ -622,17 +636,17 @@ __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
     const int md = T.mfac[n.L0];
     const int t0 = T.colptr[n.cT];
     if (!prev_wide) gsync<NT>();
-    if (md & 0x80) fac_range(T, s.W, t0, n.nnzL, md & 7, tid, NT, bad);
-    else if (inw) fac_range(T, s.W, t0, n.nnzL, md & 7, lane, 32, bad);
+    if (md & 0x80) fac_range(T, wp<FT>(s), t0, n.nnzL, md & 7, tid, NT, bad);
+    else if (inw) fac_range(T, wp<FT>(s), t0, n.nnzL, md & 7, lane, 32, bad);
     gsync<NT>();
-    if (top_inverse<NT>(s.W, T.dslot, s.tb, s.Mg, n.nT)) bad = true;
+    if (top_inverse<NT>((const FT*)wp<FT>(s), T.dslot, s.tb, s.Mg, n.nT)) bad = true;
   }
   return !gsync_or<NT>(bad);
 }
 
 // In-place (L D L^T) v = b: forward levels below the top block, the top rows'
 // right-hand side, the dense top solve, backward levels below the top block.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
@@ -643,10 +657,10 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
     const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      fwd_range(T, s.W, v, c0, c1, md & 7, tid, NT, false);
+      fwd_range(T, (const FT*)wp<FT>(s), v, c0, c1, md & 7, tid, NT, false);
       gsync<NT>();
     } else if (inw) {
-      fwd_range(T, s.W, v, c0, c1, md & 7, lane, 32, false);
+      fwd_range(T, (const FT*)wp<FT>(s), v, c0, c1, md & 7, lane, 32, false);
       __syncwarp();
     }
     prev_wide = wide;
@@ -654,8 +668,8 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
   if (n.nT > 0) {
     const int md = T.mfwd[n.L0];
     if (!prev_wide) gsync<NT>();
-    if (md & 0x80) fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, tid, NT, true);
-    else if (inw) fwd_range(T, s.W, v, n.cT, n.Nj, md & 7, lane, 32, true);
+    if (md & 0x80) fwd_range(T, (const FT*)wp<FT>(s), v, n.cT, n.Nj, md & 7, tid, NT, true);
+    else if (inw) fwd_range(T, (const FT*)wp<FT>(s), v, n.cT, n.Nj, md & 7, lane, 32, true);
     gsync<NT>();
     top_apply<NT>(s.Mg, v + n.cT, n.nT);
     prev_wide = true;
@@ -665,10 +679,10 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
     const bool wide = (md & 0x80) != 0;
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      bwd_level(T, s.W, v, lv, md & 7, tid, NT);
+      bwd_level(T, (const FT*)wp<FT>(s), v, lv, md & 7, tid, NT);
       gsync<NT>();
     } else if (inw) {
-      bwd_level(T, s.W, v, lv, md & 7, lane, 32);
+      bwd_level(T, (const FT*)wp<FT>(s), v, lv, md & 7, lane, 32);
       __syncwarp();
     }
     prev_wide = wide;
@@ -678,20 +692,20 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
 
 // x = A^{-1} rhs with `refine` refinement steps against the matrix-free A.
 // unit >= 0 means rhs = e_unit.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ void solve_refined(const DevNet& n, const TB& T, const Sh& s, const double* rhs,
                               int unit, double* x, double* t, int refine) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) x[p] = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
   gsync<NT>();
-  solve<NT>(n, T, s, x);
+  solve<NT, FT>(n, T, s, x);
   for (int it = 0; it < refine; ++it) {
     for (int p = tid; p < n.Nj; p += NT) {
       const double b = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
       t[p] = b - amul_node(n, T, s, p, x);
     }
     gsync<NT>();
-    solve<NT>(n, T, s, t);
+    solve<NT, FT>(n, T, s, t);
     for (int p = tid; p < n.Nj; p += NT) x[p] = x[p] + t[p];
     gsync<NT>();
   }
@@ -729,7 +743,7 @@ __device__ void dense_solve(double* C, double* y, int m) {
 // ---------------------------------------------------------------- assembly
 // GGA assembly (linkcoeffs -> emittercoeffs -> nodecoeffs, solver.py:2958-3007)
 // into W (pattern of L) and F = V0; Xflow saved for PRV downstream nodes.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const double* kerow,
                              const double* drow) {
   const int tid = gtid<NT>();
@@ -775,7 +789,7 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
     }
     xf = xf - drow[nd];
     F = F + xf;
-    s.W[T.colptr[p]] = dg;
+    wp<FT>(s)[T.colptr[p]] = (FT)dg;
     s.V0[p] = F;
     if (n.node_xf[p] >= 0) s.xf[n.node_xf[p]] = xf;
   }
@@ -786,9 +800,9 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       if (pl & 0x8000) continue;
       v += -s.P[pl];
     }
-    s.W[T.pslot[t]] = v;
+    wp<FT>(s)[T.pslot[t]] = (FT)v;
   }
-  for (int t = tid; t < n.nfill; t += NT) s.W[T.fill[t]] = 0.0;
+  for (int t = tid; t < n.nfill; t += NT) wp<FT>(s)[T.fill[t]] = FT(0);
   gsync<NT>();
   if (tid == 0) {  // valvecoeffs after nodecoeffs, in valve order
     for (int i = 0; i < n.npcv; ++i) {
@@ -804,10 +818,11 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       const double f1 = dy + ((act && xf2 < 0.0) ? xf2 : 0.0);
       const double f2 = -dy + n.pcv_hset[i] * kCBIG * mact;
       const int j1 = n.pcv_j1[i], j2 = n.pcv_j2[i];
-      s.W[n.pcv_off[i]] += -pna;
-      s.W[T.colptr[j1]] += pna;
-      s.W[T.colptr[j2]] += pna;
-      s.W[T.colptr[j2]] += kCBIG * mact;
+      FT* W = wp<FT>(s);
+      W[n.pcv_off[i]] += (FT)(-pna);
+      W[T.colptr[j1]] += (FT)pna;
+      W[T.colptr[j2]] += (FT)pna;
+      W[T.colptr[j2]] += (FT)(kCBIG * mact);
       s.V0[j1] += f1;
       s.V0[j2] += f2;
       s.P[k] = pna;
@@ -819,7 +834,7 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
 
 // Reduced-matrix assembly at the current state (dgga/autodiff.py:928-962):
 // every link with its P, + emh diagonal, + CBIG on ACTIVE PRV downstream nodes.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ void assemble_reduced(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) {
@@ -831,14 +846,14 @@ __device__ void assemble_reduced(const DevNet& n, const TB& T, const Sh& s) {
       const int i = n.cb_idx[c];
       dg += kCBIG * (s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0);
     }
-    s.W[T.colptr[p]] = dg;
+    wp<FT>(s)[T.colptr[p]] = (FT)dg;
   }
   for (int t = tid; t < n.npairs; t += NT) {
     double v = 0.0;
     for (int e = T.pptr[t]; e < T.pptr[t + 1]; ++e) v += -s.P[T.plink[e] & 0x7fff];
-    s.W[T.pslot[t]] = v;
+    wp<FT>(s)[T.pslot[t]] = (FT)v;
   }
-  for (int t = tid; t < n.nfill; t += NT) s.W[T.fill[t]] = 0.0;
+  for (int t = tid; t < n.nfill; t += NT) wp<FT>(s)[T.fill[t]] = FT(0);
   gsync<NT>();
 }
 
@@ -869,7 +884,7 @@ __device__ void adj_coeffs(const DevNet& n, const Sh& s, const double* rrow,
 // true M_p.  The Woodbury columns A^{-1} e_u come from one substitution each;
 // the outer refinement makes the result independent of their rounding.
 // rhs: V0 (kept), result in dH.
-template <int NT, class TB>
+template <int NT, class FT, class TB>
 __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
                              bool any_act, int refine) {
@@ -877,7 +892,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
   double* t = s.V2;
   const int tid = gtid<NT>();
   if (!any_act) {
-    solve_refined<NT>(n, T, s, rhs, -1, dH, t, refine);
+    solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, refine);
     return;
   }
   const int p = n.npcv, m = 2 * p;
@@ -897,7 +912,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
       if (actf[i] != 0.0) rp[n.pcv_j2[i]] = -rprv[i];
   }
   gsync<NT>();
-  solve_refined<NT>(n, T, s, rp, -1, dH, t, refine);
+  solve_refined<NT, FT>(n, T, s, rp, -1, dH, t, refine);
   for (int c = 0; c < m; ++c) {
     // columns of inactive valves meet y = 0 in the correction: zero, not solved
     if (actf[c < p ? c : c - p] == 0.0) {
@@ -906,7 +921,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
       continue;
     }
     const int u = c < p ? n.pcv_j2[c] : n.pcv_j1[c - p];
-    solve_refined<NT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
+    solve_refined<NT, FT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
   }
   if (tid == 0) {
     // C = [R2 ; I2 - CBIG R2], rows of inactive valves -> identity
@@ -956,7 +971,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
         if (actf[i] != 0.0) res[n.pcv_j2[i]] = rp[n.pcv_j2[i]] - dH[n.pcv_j2[i]];
     }
     gsync<NT>();
-    solve_refined<NT>(n, T, s, res, -1, sx, t, refine);
+    solve_refined<NT, FT>(n, T, s, res, -1, sx, t, refine);
     wood(sx, res);
     for (int q = tid; q < n.Nj; q += NT) dH[q] = dH[q] + sx[q];
     gsync<NT>();
@@ -972,7 +987,13 @@ __device__ Sh carve(const DevNet& n, unsigned char* base) {
   s.q = nullptr;  // link flows and Y live in the global workspace (set by the kernel)
   s.Y = nullptr;
   s.P = (double*)take(8ull * n.L);
-  s.W = (double*)take(8ull * n.nnzL);
+  if (n.fp32) {
+    s.Wf = (float*)take(4ull * n.nnzL);
+    s.W = nullptr;
+  } else {
+    s.W = (double*)take(8ull * n.nnzL);
+    s.Wf = nullptr;
+  }
   s.V0 = (double*)take(8ull * n.Nj);
   s.V1 = (double*)take(8ull * n.Nj);
   s.V2 = (double*)take(8ull * n.Nj);
@@ -997,7 +1018,7 @@ size_t smem_bytes(const DevNet& n) {
   auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
   size_t o = 0;
   o += a16(8ull * n.L);
-  o += a16(8ull * n.nnzL);
+  o += a16((n.fp32 ? 4ull : 8ull) * n.nnzL);
   o += 3 * a16(8ull * n.Nj);
   o += 3 * a16(8ull * n.emcap);
   o += a16(8ull * (n.Nf > 0 ? n.Nf : 1));
@@ -1055,7 +1076,7 @@ __device__ bool build_emitters(const DevNet& n, const Sh& s, const double* val, 
 }
 
 // ---------------------------------------------------------------- forward kernel
-template <int NT, int GR, class TB>
+template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
                                                         int state_bytes) {
   const int groups = GR;
@@ -1113,13 +1134,13 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
       s.Y[k] = Y;
     }
     gsync<NT>();
-    assemble_gga<NT>(n, T, s, kerow, drow);
-    if (!factor<NT>(n, T, s)) {
+    assemble_gga<NT, FT>(n, T, s, kerow, drow);
+    if (!factor<NT, FT>(n, T, s)) {
       info = WDS_INFO_NOT_PD;
       iters = it;
       break;
     }
-    solve_refined<NT>(n, T, s, s.V0, -1, s.V1, s.V2, a.refine);
+    solve_refined<NT, FT>(n, T, s, s.V0, -1, s.V1, s.V2, a.refine);
     // ---- newflows (hydsolver.c:358-514 as restated in solver.py:3092-3110)
     double sums[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k = gtid<NT>(); k < n.L; k += NT) {
@@ -1241,8 +1262,8 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
     for (int step = 0; step <= a.polish; ++step) {
       adj_coeffs<NT>(n, s, rrow, kerow);
-      assemble_reduced<NT>(n, T, s);
-      if (!factor<NT>(n, T, s)) {
+      assemble_reduced<NT, FT>(n, T, s);
+      if (!factor<NT, FT>(n, T, s)) {
         info = WDS_INFO_NOT_PD;
         break;
       }
@@ -1285,7 +1306,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
         s.V0[p] = (mm - bt) + emh * re;
       }
       gsync<NT>();
-      primal_solve<NT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act, a.refine);
+      primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act, a.refine);
       // dq, de, state update
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
@@ -1311,8 +1332,8 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
       gsync<NT>();
     }
     if (info == 0) {  // store the terminal state for the adjoint
-      double* Wt = w.W + (size_t)b * n.nnzL;
-      for (int t = gtid<NT>(); t < n.nnzL; t += NT) Wt[t] = s.W[t];
+      FT* Wt = reinterpret_cast<FT*>(w.W) + (size_t)b * n.nnzL;
+      for (int t = gtid<NT>(); t < n.nnzL; t += NT) Wt[t] = wp<FT>(s)[t];
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double q = s.q[k];
         w.P[(size_t)b * n.L + k] = s.P[k];
@@ -1380,7 +1401,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
 // ---------------------------------------------------------------- adjoint kernel
 // Node adjoint with constraint rows (autodiff.py:1107-1154) and the
 // theta contraction (autodiff.py:1246-1312).
-template <int NT, int GR, class TB>
+template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
                                                         int state_bytes) {
   const int groups = GR;
@@ -1403,8 +1424,8 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
   }
   s.Mg = w.M + (size_t)b * n.nT * n.nT;  // terminal top-block inverse of the forward
   if (!w.valid[b]) return;  // uniform per group
-  const double* Wt = w.W + (size_t)b * n.nnzL;
-  for (int t = gtid<NT>(); t < n.nnzL; t += NT) s.W[t] = Wt[t];
+  const FT* Wt = reinterpret_cast<const FT*>(w.W) + (size_t)b * n.nnzL;
+  for (int t = gtid<NT>(); t < n.nnzL; t += NT) wp<FT>(s)[t] = Wt[t];
   for (int k = gtid<NT>(); k < n.L; k += NT) s.P[k] = w.P[(size_t)b * n.L + k];
   const int pc = n.npcv > 0 ? n.npcv : 1;
   // status is only consulted for ACTIVE flags of PRVs
@@ -1445,7 +1466,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
   double* lam = s.V1;
   double* t = s.V2;
   if (!any_act) {
-    solve_refined<NT>(n, T, s, s.V0, -1, lam, t, 2);
+    solve_refined<NT, FT>(n, T, s, s.V0, -1, lam, t, 2);
   } else {
     const int p = n.npcv;
     double* scr = w.scr + (size_t)b * w.nscr * n.Nj;
@@ -1464,14 +1485,14 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
       for (int i = 0; i < p; ++i)
         if (actf[i] != 0.0) r2[n.pcv_j2[i]] = gQ[n.pcv_link[i]];
     gsync<NT>();
-    solve_refined<NT>(n, T, s, r2, -1, lam, t, 2);
+    solve_refined<NT, FT>(n, T, s, r2, -1, lam, t, 2);
     for (int c = 0; c < p; ++c) {
       if (actf[c] == 0.0) {  // meets y = 0 in the correction
         for (int q = gtid<NT>(); q < n.Nj; q += NT) cols[(size_t)c * n.Nj + q] = 0.0;
         gsync<NT>();
         continue;
       }
-      solve_refined<NT>(n, T, s, nullptr, n.pcv_j2[c], cols + (size_t)c * n.Nj, t, 0);
+      solve_refined<NT, FT>(n, T, s, nullptr, n.pcv_j2[c], cols + (size_t)c * n.Nj, t, 0);
     }
     if (gtid<NT>() == 0)
       for (int a0 = 0; a0 < p; ++a0)
@@ -1505,7 +1526,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
           if (actf[i] != 0.0)
             res[n.pcv_j2[i]] = r2[n.pcv_j2[i]] - (lam[n.pcv_j2[i]] - lam[n.pcv_j1[i]]);
       gsync<NT>();
-      solve_refined<NT>(n, T, s, res, -1, sx, t, 2);
+      solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 2);
       wood(sx, res);
       for (int q = gtid<NT>(); q < n.Nj; q += NT) lam[q] = lam[q] + sx[q];
       gsync<NT>();
@@ -1567,9 +1588,14 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int grou
   const int st = (int)smem_bytes(n);
   const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
   void (*kern)(DevNet, DevWork, FwdArgs, int) =
-      n.wide ? k_forward<256, 1, LTab>
-      : groups == 1 ? k_forward<256, 1, STab> : groups == 2 ? k_forward<256, 2, STab>
-      : groups == 3 ? k_forward<256, 3, STab> : k_forward<256, 4, STab>;
+      n.fp32 ? (n.wide ? k_forward<256, 1, LTab, float>
+                : groups == 1 ? k_forward<256, 1, STab, float>
+                : groups == 2 ? k_forward<256, 2, STab, float>
+                : groups == 3 ? k_forward<256, 3, STab, float> : k_forward<256, 4, STab, float>)
+             : (n.wide ? k_forward<256, 1, LTab, double>
+                : groups == 1 ? k_forward<256, 1, STab, double>
+                : groups == 2 ? k_forward<256, 2, STab, double>
+                : groups == 3 ? k_forward<256, 3, STab, double> : k_forward<256, 4, STab, double>);
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward: ") + cudaGetErrorString(ce);
@@ -1594,9 +1620,14 @@ int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int grou
   const int st = (int)smem_bytes(n);
   const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
   void (*kern)(DevNet, DevWork, AdjArgs, int) =
-      n.wide ? k_adjoint<256, 1, LTab>
-      : groups == 1 ? k_adjoint<256, 1, STab> : groups == 2 ? k_adjoint<256, 2, STab>
-      : groups == 3 ? k_adjoint<256, 3, STab> : k_adjoint<256, 4, STab>;
+      n.fp32 ? (n.wide ? k_adjoint<256, 1, LTab, float>
+                : groups == 1 ? k_adjoint<256, 1, STab, float>
+                : groups == 2 ? k_adjoint<256, 2, STab, float>
+                : groups == 3 ? k_adjoint<256, 3, STab, float> : k_adjoint<256, 4, STab, float>)
+             : (n.wide ? k_adjoint<256, 1, LTab, double>
+                : groups == 1 ? k_adjoint<256, 1, STab, double>
+                : groups == 2 ? k_adjoint<256, 2, STab, double>
+                : groups == 3 ? k_adjoint<256, 3, STab, double> : k_adjoint<256, 4, STab, double>);
   cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (ce != cudaSuccess) {
     *err = std::string("wds_adjoint: ") + cudaGetErrorString(ce);

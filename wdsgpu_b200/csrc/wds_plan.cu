@@ -552,6 +552,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   dsz.N = N; dsz.L = L; dsz.Nj = Nj; dsz.Nf = Nf; dsz.nnzL = nnzL; dsz.npcv = npcv;
   dsz.nxf = nxf; dsz.nT = nT;
   dsz.emcap = std::min(Nj, net->emitter_capacity > 0 ? net->emitter_capacity : 64);
+  dsz.fp32 = net->factor_fp32 ? 1 : 0;
   const size_t state_bytes = state_smem_bytes(dsz);
   Blob sblob;
   TabOff to{};
@@ -631,6 +632,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.tl_hmin = P_(double, o_tln); d.tl_flags = P_(uint8_t, o_tlf);
   d.stab = P_(uint4, o_stab);
   d.wide = wide ? 1 : 0;
+  d.fp32 = net->factor_fp32 ? 1 : 0;
   d.stab_bytes = wide ? 0 : (int)stab_bytes.size();  // staged into shared memory (narrow only)
   d.o_spair = to.sp; d.o_fpair = to.fp; d.o_colptr = to.cp;
   d.o_rowidx = to.ri; d.o_levptr = to.lp; d.o_rptr = to.rp;

@@ -38,7 +38,7 @@ import torch
 
 from . import _lib
 from .autodiff import _adjoint_guards
-from .solver import GGASolver, _check_emitter_cap
+from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
 
 __all__ = ["eps_solve", "EpsSM100", "tank_links"]
 
@@ -113,8 +113,8 @@ def _step_forward(s, d, rh, ke, r, B, max_iter, acc, polish, q0, e0):
     if bool((info != 0).any()):
         bad = torch.nonzero(info != 0).flatten().tolist()
         if bool((info & _lib.INFO_NOT_PD).any()):
-            raise RuntimeError("eps: the node matrix of scenarios %s is not positive definite"
-                               % bad[:8])
+            raise RuntimeError("eps: the node matrix of scenarios %s is not positive definite%s"
+                               % (bad[:8], _not_pd_hint(s)))
         raise RuntimeError("eps: scenarios %s did not converge (relerr=%s > accuracy=%g)"
                            % (bad[:8], [float(o["relerr"][b]) for b in bad[:4]], acc))
     return o

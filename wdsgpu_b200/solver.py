@@ -75,6 +75,9 @@ class _Plan:
         net.emitter_capacity = int(solver.emitter_capacity)
         net.layout = {"auto": _lib.LAYOUT_AUTO, "shared": _lib.LAYOUT_SHARED,
                       "global": _lib.LAYOUT_GLOBAL}[solver.sm100_layout]
+        if solver.sm100_factor_dtype not in (torch.float64, torch.float32):
+            raise ValueError("sm100_factor_dtype must be torch.float64 or torch.float32")
+        net.factor_fp32 = 1 if solver.sm100_factor_dtype == torch.float32 else 0
         with torch.cuda.device(self.device):
             _lib.check(lib.wds_plan(ctypes.byref(net), self.max_batch,
                                     ctypes.byref(self.handle)), "wds_plan")
@@ -113,6 +116,14 @@ class _Plan:
             pass
 
 
+def _not_pd_hint(solver):
+    """Suffix of a not-positive-definite error in FP32-factor mode."""
+    if getattr(solver, "sm100_factor_dtype", torch.float64) == torch.float32:
+        return (" (sm100_factor_dtype=float32: the FP32 LDL^T lost positive "
+                "definiteness on this ill-conditioned node matrix; use float64)")
+    return ""
+
+
 def _check_emitter_cap(solver, info):
     cap = torch.nonzero(info & _lib.INFO_EMITTER_CAP).flatten()
     if cap.numel():
@@ -141,6 +152,11 @@ class GGASolver:
     says where the schedule tables and per-scenario state live: shared memory
     (several scenarios per SM), or global memory for networks too large for
     it ("auto" picks shared memory when it fits).
+    `sm100_factor_dtype` (torch.float64 or torch.float32, set before the first
+    solve): precision of the LDL^T factor and of the substitutions; with
+    float32 every linear solve is refined against the FP64 operator
+    (`sm100_refine` steps), and residuals, headloss, convergence test, status
+    decisions and the adjoint right-hand side stay FP64.
     """
 
     def __init__(self, net, device="cuda", dtype=torch.float64, mode="dense",
@@ -163,6 +179,7 @@ class GGASolver:
         self.net = net
         self.sm100_refine = 2
         self.sm100_layout = "auto"
+        self.sm100_factor_dtype = torch.float64
         # emitters per scenario kept in shared memory (junctions with Ke > 0)
         self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
         lt = np.asarray(net.link_type, dtype=np.int64)
@@ -548,7 +565,7 @@ class GGASolver:
         if bad.numel():
             raise RuntimeError(
                 "batched LDL^T failed: the node matrix of scenarios %s is not "
-                "positive definite" % bad.tolist())
+                "positive definite%s" % (bad.tolist(), _not_pd_hint(self)))
         out = dict(head_ft=o["head"], flow_cfs=o["flow"], emitter_cfs=o["emit"],
                    iters=o["iters"].to(torch.int64), relerr=o["relerr"],
                    converged=(info == 0))
