@@ -179,6 +179,45 @@ int wds_plan_stats(const WdsPlan* plan, int64_t* out8);
 int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
                       int32_t* rowidx, int32_t* parent, int32_t* level);
 
+/* Device arrays of one plan in a multi-plan call (shapes as in wds_forward /
+ * wds_adjoint). */
+typedef struct WdsForwardIO {
+  const double* demand;
+  const double* fixed_head;
+  const double* ke;
+  const double* r;
+  double* head;
+  double* flow;
+  double* emitter;
+  int8_t* status;
+  int32_t* iters;
+  double* relerr;
+  int32_t* info;
+} WdsForwardIO;
+
+typedef struct WdsAdjointIO {
+  const double* gH;
+  const double* gQ;
+  const double* gE;
+  double* gd;
+  double* grh;
+  double* gke;
+  double* gr;
+} WdsAdjointIO;
+
+/* Networks of different sizes in one launch: `nplans` (at most 8) plans, each
+ * with its own batch, options and arrays, run by one persistent kernel whose
+ * CTAs are split among the plans (shared-memory or large-network layout per
+ * plan).  Same per-plan results as wds_forward; no counterpart in the
+ * reference, whose solver holds one network (dgga/solver.py:160). */
+int wds_forward_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batch,
+                      const WdsForwardOpts* opts, const WdsForwardIO* io, void* stream);
+
+/* Adjoint of the last implicit wds_forward_multi (or wds_forward) of every
+ * plan, in one launch; per plan as wds_adjoint. */
+int wds_adjoint_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batch,
+                      const WdsAdjointIO* io, void* stream);
+
 /* Size of the fixed device array used by wds_forward_noalloc (64 MiB). */
 #define WDS_NOALLOC_SCRATCH_BYTES (64u << 20)
 

@@ -35,7 +35,9 @@ def test_struct_layout_matches_header(tmp_path):
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "wds_b200.h"',
              'int main(void){',
              'printf("%zu\\n", sizeof(WdsNetwork));',
-             'printf("%zu\\n", sizeof(WdsForwardOpts));']
+             'printf("%zu\\n", sizeof(WdsForwardOpts));',
+             'printf("%zu\\n", sizeof(WdsForwardIO));',
+             'printf("%zu\\n", sizeof(WdsAdjointIO));']
     lines += ['printf("%%zu\\n", offsetof(WdsNetwork, %s));' % f for f in fields]
     lines += ['printf("%%zu\\n", offsetof(WdsForwardOpts, %s));' % f for f in ofields]
     lines += ['return 0;}']
@@ -46,6 +48,9 @@ def test_struct_layout_matches_header(tmp_path):
                                            check=True).stdout.split()]
     assert vals[0] == ctypes.sizeof(_lib.WdsNetwork)
     assert vals[1] == ctypes.sizeof(_lib.WdsForwardOpts)
+    assert vals[2] == ctypes.sizeof(_lib.WdsForwardIO)
+    assert vals[3] == ctypes.sizeof(_lib.WdsAdjointIO)
+    vals = vals[:2] + vals[4:]
     offs = vals[2:2 + len(fields)]
     for f, o in zip(fields, offs):
         assert getattr(_lib.WdsNetwork, f).offset == o, f

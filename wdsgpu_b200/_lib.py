@@ -24,7 +24,9 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
            -4: "unsupported network", -5: "no forward state"}
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
-           "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc")
+           "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc",
+           "wds_forward_multi", "wds_adjoint_multi")
+MULTI_MAX = 8
 
 
 class WdsNetwork(ctypes.Structure):
@@ -63,6 +65,16 @@ class WdsForwardOpts(ctypes.Structure):
     ]
 
 
+class WdsForwardIO(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "demand", "fixed_head", "ke", "r", "head", "flow", "emitter", "status", "iters",
+        "relerr", "info")]
+
+
+class WdsAdjointIO(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("gH", "gQ", "gE", "gd", "grh", "gke", "gr")]
+
+
 _lib = None
 
 
@@ -85,6 +97,13 @@ def load():
     lib.wds_forward_noalloc.restype = ctypes.c_int
     lib.wds_adjoint.argtypes = [vp, ctypes.c_int32] + [vp] * 7 + [vp]
     lib.wds_adjoint.restype = ctypes.c_int
+    lib.wds_forward_multi.argtypes = [ctypes.c_int32, ctypes.POINTER(vp), c_int32_p,
+                                      ctypes.POINTER(WdsForwardOpts),
+                                      ctypes.POINTER(WdsForwardIO), vp]
+    lib.wds_forward_multi.restype = ctypes.c_int
+    lib.wds_adjoint_multi.argtypes = [ctypes.c_int32, ctypes.POINTER(vp), c_int32_p,
+                                      ctypes.POINTER(WdsAdjointIO), vp]
+    lib.wds_adjoint_multi.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]
     lib.wds_plan_stats.restype = ctypes.c_int
     lib.wds_plan_symbolic.argtypes = [vp] + [c_int32_p] * 5

@@ -170,4 +170,31 @@ int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int grou
                    void* stream, std::string* err);
 size_t state_smem_bytes(const DevNet& n);
 
+// One plan's share of a multi-plan launch.  `groups` is the number of
+// scenario groups (256 threads each) per 768-thread CTA; state_bytes and cta0
+// are filled by the launcher.
+struct FwdJob {
+  DevNet n;
+  DevWork w;
+  FwdArgs a;
+  int groups, state_bytes, cta0;
+};
+struct AdjJob {
+  DevNet n;
+  DevWork w;
+  AdjArgs a;
+  int groups, state_bytes, cta0;
+};
+constexpr int WDS_MULTI_MAX = 8;  // plans per multi-plan launch
+struct FwdJobs {
+  FwdJob j[WDS_MULTI_MAX];
+  int n;
+};
+struct AdjJobs {
+  AdjJob j[WDS_MULTI_MAX];
+  int n;
+};
+int launch_forward_multi(FwdJobs& jobs, void* stream, std::string* err);
+int launch_adjoint_multi(AdjJobs& jobs, void* stream, std::string* err);
+
 }  // namespace wds

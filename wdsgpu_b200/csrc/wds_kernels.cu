@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <string>
+#include <algorithm>
 #include <type_traits>
 
 #include "wds_internal.h"
@@ -1076,18 +1077,19 @@ __device__ bool build_emitters(const DevNet& n, const Sh& s, const double* val, 
 }
 
 // ---------------------------------------------------------------- forward kernel
-template <int NT, int GR, class TB, class FT>
-__global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
-                                                        int state_bytes) {
-  const int groups = GR;
+// Forward of one CTA (block `blk` of the plan, `groups` scenario groups of NT
+// threads; groups beyond it, in a CTA with more threads, stay idle).
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, const FwdArgs& a,
+                                             int state_bytes, int blk, int groups) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / NT;
-  const int b = blockIdx.x * groups + g;
+  const int b = blk * groups + g;
   TB T;
   Sh s;
   if constexpr (TB::kWide) {
     // large network: tables and scenario state stay in global memory
-    if (b >= a.B) return;
+    if (g >= groups || b >= a.B) return;
     T = tab_view<TB>(n, (const unsigned char*)n.stab);
     s = carve(n, w.state + (size_t)b * state_bytes);
   } else {
@@ -1096,7 +1098,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
       ((uint4*)smem_raw)[i] = n.stab[i];
     __syncthreads();
     T = tab_view<TB>(n, smem_raw);
-    if (b >= a.B) return;  // a whole group; other groups use their own barrier
+    if (g >= groups || b >= a.B) return;  // a whole group; groups use their own barriers
     s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   }
   s.q = w.lk + (size_t)b * 2 * n.L;
@@ -1401,17 +1403,17 @@ __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, Fwd
 // ---------------------------------------------------------------- adjoint kernel
 // Node adjoint with constraint rows (autodiff.py:1107-1154) and the
 // theta contraction (autodiff.py:1246-1312).
-template <int NT, int GR, class TB, class FT>
-__global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
-                                                        int state_bytes) {
-  const int groups = GR;
+// Adjoint of one CTA (as forward_body).
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, const AdjArgs& a,
+                                             int state_bytes, int blk, int groups) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / NT;
-  const int b = blockIdx.x * groups + g;
+  const int b = blk * groups + g;
   TB T;
   Sh s;
   if constexpr (TB::kWide) {
-    if (b >= a.B) return;
+    if (g >= groups || b >= a.B) return;
     T = tab_view<TB>(n, (const unsigned char*)n.stab);
     s = carve(n, w.state + (size_t)b * state_bytes);
   } else {
@@ -1419,7 +1421,7 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
       ((uint4*)smem_raw)[i] = n.stab[i];
     __syncthreads();
     T = tab_view<TB>(n, smem_raw);
-    if (b >= a.B) return;
+    if (g >= groups || b >= a.B) return;
     s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   }
   s.Mg = w.M + (size_t)b * n.nT * n.nT;  // terminal top-block inverse of the forward
@@ -1575,9 +1577,118 @@ __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, Adj
   }
 }
 
+template <int NT, int GR, class TB, class FT>
+__global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
+                                                        int state_bytes) {
+  forward_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, GR);
+}
+
+template <int NT, int GR, class TB, class FT>
+__global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
+                                                        int state_bytes) {
+  adjoint_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, GR);
+}
+
+// Several plans (networks of different sizes) in one launch: CTAs
+// [job.cta0, next job's cta0) run the job's plan, with 3 groups of 256
+// threads each (a plan that fits fewer groups in shared memory leaves the
+// others idle; large-network plans run 3 scenarios per CTA from global memory).
+template <class FT>
+__global__ void __launch_bounds__(768, 1) k_forward_multi(const __grid_constant__ FwdJobs jobs) {
+  int p = 0;
+  while (p + 1 < jobs.n && (int)blockIdx.x >= jobs.j[p + 1].cta0) ++p;
+  const FwdJob& J = jobs.j[p];
+  if (J.n.wide)
+    forward_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+  else
+    forward_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+}
+
+template <class FT>
+__global__ void __launch_bounds__(768, 1) k_adjoint_multi(const __grid_constant__ AdjJobs jobs) {
+  int p = 0;
+  while (p + 1 < jobs.n && (int)blockIdx.x >= jobs.j[p + 1].cta0) ++p;
+  const AdjJob& J = jobs.j[p];
+  if (J.n.wide)
+    adjoint_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+  else
+    adjoint_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+}
+
 }  // namespace
 
 size_t state_smem_bytes(const DevNet& n) { return smem_bytes(n); }
+
+template <class Jobs>
+static size_t multi_smem(const Jobs& jobs) {
+  size_t smem = 0;
+  for (int p = 0; p < jobs.n; ++p) {
+    const auto& J = jobs.j[p];
+    if (!J.n.wide)
+      smem = std::max(smem, (size_t)J.n.stab_bytes + (size_t)J.groups * (size_t)J.state_bytes);
+  }
+  return smem;
+}
+
+int launch_forward_multi(FwdJobs& jobs, void* stream, std::string* err) {
+  int ctas = 0;
+  bool fp32 = false;
+  for (int p = 0; p < jobs.n; ++p) {
+    FwdJob& J = jobs.j[p];
+    if (J.n.npcv > 4) {
+      *err = "wds_forward_multi: more than 4 status-machine PRVs is not supported by this build";
+      return WDS_E_UNSUPPORTED;
+    }
+    if (p > 0 && (J.n.fp32 != 0) != fp32) {
+      *err = "wds_forward_multi: the plans mix FP32 and FP64 factors";
+      return WDS_E_ARG;
+    }
+    fp32 = J.n.fp32 != 0;
+    J.state_bytes = (int)smem_bytes(J.n);
+    J.cta0 = ctas;
+    ctas += (J.a.B + J.groups - 1) / J.groups;
+  }
+  const size_t smem = multi_smem(jobs);
+  void (*kern)(FwdJobs) = fp32 ? k_forward_multi<float> : k_forward_multi<double>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce == cudaSuccess && ctas > 0) {
+    kern<<<ctas, 768, smem, (cudaStream_t)stream>>>(jobs);
+    ce = cudaGetLastError();
+  }
+  if (ce != cudaSuccess) {
+    *err = std::string("wds_forward_multi: ") + cudaGetErrorString(ce);
+    return WDS_E_CUDA;
+  }
+  return WDS_OK;
+}
+
+int launch_adjoint_multi(AdjJobs& jobs, void* stream, std::string* err) {
+  int ctas = 0;
+  bool fp32 = false;
+  for (int p = 0; p < jobs.n; ++p) {
+    AdjJob& J = jobs.j[p];
+    if (p > 0 && (J.n.fp32 != 0) != fp32) {
+      *err = "wds_adjoint_multi: the plans mix FP32 and FP64 factors";
+      return WDS_E_ARG;
+    }
+    fp32 = J.n.fp32 != 0;
+    J.state_bytes = (int)smem_bytes(J.n);
+    J.cta0 = ctas;
+    ctas += (J.a.B + J.groups - 1) / J.groups;
+  }
+  const size_t smem = multi_smem(jobs);
+  void (*kern)(AdjJobs) = fp32 ? k_adjoint_multi<float> : k_adjoint_multi<double>;
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce == cudaSuccess && ctas > 0) {
+    kern<<<ctas, 768, smem, (cudaStream_t)stream>>>(jobs);
+    ce = cudaGetLastError();
+  }
+  if (ce != cudaSuccess) {
+    *err = std::string("wds_adjoint_multi: ") + cudaGetErrorString(ce);
+    return WDS_E_CUDA;
+  }
+  return WDS_OK;
+}
 
 int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
                    void* stream, std::string* err) {

@@ -753,6 +753,78 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   return WDS_OK;
 }
 
+extern "C" int wds_forward_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batch,
+                                 const WdsForwardOpts* opts, const WdsForwardIO* io,
+                                 void* stream) {
+  using namespace wds;
+  if (nplans <= 0 || nplans > WDS_MULTI_MAX || !plans || !batch || !opts || !io)
+    return fail(WDS_E_ARG, "wds_forward_multi: bad argument (1 to 8 plans)");
+  FwdJobs jobs{};
+  jobs.n = nplans;
+  for (int p = 0; p < nplans; ++p) {
+    const WdsPlan* plan = plans[p];
+    const WdsForwardOpts* o = &opts[p];
+    const WdsForwardIO& x = io[p];
+    if (!plan || batch[p] <= 0 || batch[p] > plan->max_batch)
+      return fail(WDS_E_ARG, "wds_forward_multi: plan " + std::to_string(p) +
+                                 ": bad plan or batch beyond its max_batch");
+    if (!x.demand || !x.fixed_head || !x.ke || !x.r || !x.head || !x.flow || !x.emitter ||
+        !x.status || !x.iters || !x.relerr || !x.info)
+      return fail(WDS_E_ARG, "wds_forward_multi: plan " + std::to_string(p) + ": null pointer");
+    if (o->max_iter <= 0 || !(o->accuracy > 0.0) || o->refine < 0)
+      return fail(WDS_E_ARG, "wds_forward_multi: plan " + std::to_string(p) + ": bad options");
+    for (int q = 0; q < p; ++q)
+      if (plans[q] == plan)
+        return fail(WDS_E_ARG, "wds_forward_multi: a plan appears twice (its workspace would be shared)");
+    FwdJob& J = jobs.j[p];
+    J.n = plan->dn;
+    J.w = plan->dw;
+    J.groups = plan->dn.wide ? 3 : std::min(3, plan->groups);
+    FwdArgs& a = J.a;
+    a.B = batch[p]; a.hacc = o->accuracy; a.max_iter = o->max_iter;
+    a.sm = o->status_machine ? 1 : 0; a.refine = o->refine; a.polish = o->polish_steps;
+    a.ke_stride = o->ke_stride; a.r_stride = o->r_stride;
+    a.d = x.demand; a.rh = x.fixed_head; a.ke = x.ke; a.r = x.r; a.q0 = o->q0; a.e0 = o->e0;
+    a.head = x.head; a.flow = x.flow; a.emit = x.emitter; a.status = x.status;
+    a.iters = x.iters; a.relerr = x.relerr; a.info = x.info;
+  }
+  std::string err;
+  const int rc = launch_forward_multi(jobs, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  for (int p = 0; p < nplans; ++p) {
+    plans[p]->have_state = opts[p].polish_steps >= 0;
+    plans[p]->state_batch = batch[p];
+  }
+  return WDS_OK;
+}
+
+extern "C" int wds_adjoint_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batch,
+                                 const WdsAdjointIO* io, void* stream) {
+  using namespace wds;
+  if (nplans <= 0 || nplans > WDS_MULTI_MAX || !plans || !batch || !io)
+    return fail(WDS_E_ARG, "wds_adjoint_multi: bad argument (1 to 8 plans)");
+  AdjJobs jobs{};
+  jobs.n = nplans;
+  for (int p = 0; p < nplans; ++p) {
+    const WdsPlan* plan = plans[p];
+    const WdsAdjointIO& x = io[p];
+    if (!plan || batch[p] <= 0 || !x.gH || !x.gQ || !x.gE || !x.gd || !x.grh || !x.gke || !x.gr)
+      return fail(WDS_E_ARG, "wds_adjoint_multi: plan " + std::to_string(p) + ": bad argument");
+    if (!plan->have_state || batch[p] != plan->state_batch)
+      return fail(WDS_E_STATE, "wds_adjoint_multi: plan " + std::to_string(p) +
+                                   ": no implicit forward of this batch size to differentiate");
+    AdjJob& J = jobs.j[p];
+    J.n = plan->dn;
+    J.w = plan->dw;
+    J.groups = plan->dn.wide ? 3 : std::min(3, plan->groups);
+    J.a = AdjArgs{batch[p], x.gH, x.gQ, x.gE, x.gd, x.grh, x.gke, x.gr};
+  }
+  std::string err;
+  const int rc = launch_adjoint_multi(jobs, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  return WDS_OK;
+}
+
 extern "C" int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH, const double* gQ,
                            const double* gE, double* gd, double* grh, double* gke, double* gr,
                            void* stream) {
