@@ -8,6 +8,12 @@ sensor junctions, and the gradients w.r.t. demand, pipe roughness (chain rule
 through r = 4.727 L / C^1.852 / D^4.871) and emitter coefficients.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sm100|reference]
+    python bench.py --workload mixed|eps      (secondary workloads, one GPU)
+
+`--workload mixed`: 256 instances drawn uniformly from four networks (100,
+542 with 79 TCVs, 782 with 3 PRVs, 3000 junctions), forward + adjoint in one
+multi-plan launch per pass.  `--workload eps`: 24 hourly steps of the
+20 000-junction pump/tank network, B=64, forward + adjoint through time.
 
 N > 1 is launched with torch.distributed.run: every rank solves its own
 batch of 1024 scenarios (weak scaling); the batch-summed roughness and
@@ -209,6 +215,95 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ secondary workloads
+def run_secondary(args):
+    """Mixed-size one-launch and extended-period workloads: one JSON line."""
+    import torch
+    from wdsgpu_b200 import synth
+    from wdsgpu_b200.solver import GGASolver
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    if args.workload == "mixed":
+        from wdsgpu_b200.multi import implicit_solve_multi
+        nets = synth.config3_networks()
+        counts = np.bincount(np.random.default_rng(3).integers(0, 4, 256), minlength=4)
+        solvers = [GGASolver(n, device=dev, dense_status_machine=True) for n in nets]
+        data = []
+        for i, (n, c) in enumerate(zip(nets, counts)):
+            d, _ = synth.config2_scenarios(n, int(c), seed=50 + i, sigma=0.3)
+            rh = np.broadcast_to(np.nan_to_num(n.fixed_head_ft_at(0)), d.shape).copy()
+            data.append((torch.as_tensor(d, device=dev), torch.as_tensor(rh, device=dev)))
+        sens = [torch.as_tensor(synth.sensor_nodes(n, 8), device=dev) for n in nets]
+
+        def step():
+            Ds = [d.clone().requires_grad_(True) for d, _ in data]
+            outs = implicit_solve_multi(solvers, Ds, [rh for _, rh in data], accuracy=ACCURACY)
+            loss = sum((h[:, sv] ** 2).sum() for (h, _, _), sv in zip(outs, sens))
+            loss.backward()
+            return sum(float(D.grad.abs().sum()) for D in Ds)
+
+        units = int(counts.sum())
+        metric = ("mixed-size fwd+adjoint instances/s (256 instances of 100/542/782/3000-junction "
+                  "networks, one multi-plan launch per pass)")
+        unit = "instances/s"
+        cfg = {"workload": "mixed-size: networks of 100 jn/120 pipes, 542 jn/554 links with 79 TCVs, "
+                           "782 jn/905 pipes/3 PRVs, 3000 jn/3600 pipes; instances per network %s; "
+                           "lognormal(0.3) demands" % counts.tolist(),
+               "instances": units, "launches_per_step": 2}
+    else:
+        from wdsgpu_b200.eps import eps_solve
+        net0 = synth.config5_network()
+        pre = synth.tanks_as_junctions(net0)
+        s0 = GGASolver(pre, device=dev, dense_status_machine=True)
+        o = s0.solve(pre.demand_cfs_at(0)[None] * synth.diurnal(0.0),
+                     np.nan_to_num(pre.fixed_head_ft_at(0))[None], status_machine=True,
+                     accuracy=1e-8)
+        ctr = o["head_ft"][0].cpu().numpy()[np.asarray(net0.tank_node)]
+        net = synth.config5_network(tank_center_ft=ctr)
+        s = GGASolver(net, device=dev, dense_status_machine=True)
+        B, T = 64, 24
+        dem = torch.as_tensor(synth.eps_demands(net, T, B, seed=6), device=dev)
+        sens = torch.arange(0, net.N, 200, device=dev)
+
+        def step():
+            D = dem.clone().requires_grad_(True)
+            out = eps_solve(s, D, accuracy=ACCURACY)
+            loss = (out["head"][:, :, sens] ** 2).sum() + (out["tank_head"][-1] ** 2).sum()
+            loss.backward()
+            return float(D.grad.abs().sum())
+
+        units = B * T
+        metric = "EPS fwd+adjoint scenario-steps/s (20 000 jn, 24 hourly steps, B=64)"
+        unit = "scenario-steps/s"
+        cfg = {"workload": "extended period: about 20 000 junctions / 23 000 pipes, 4 pumps, "
+                           "3 tanks, 1 reservoir; 24 hourly steps; B=64 diurnal x lognormal(0.15) "
+                           "demands; adjoint through time with per-step recomputation",
+               "B": B, "steps_per_run": T, "layout": "global (large network)"}
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(None) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    ms = sum(times) / len(times)
+    cfg["l2"] = "flushed between steps (256 MB write, outside the timed events)"
+    line = {"metric": metric, "value": units / (ms / 1000.0), "unit": unit, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ GPU leg
 def main():
     ap = argparse.ArgumentParser()
@@ -218,9 +313,13 @@ def main():
     ap.add_argument("--impl", default="sm100", choices=("sm100", "reference"))
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config2", choices=("config2", "mixed", "eps"))
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload != "config2":
+        run_secondary(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
