@@ -179,6 +179,18 @@ int wds_plan_stats(const WdsPlan* plan, int64_t* out8);
 int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
                       int32_t* rowidx, int32_t* parent, int32_t* level);
 
+/* Several adjoints per kept scenario, on the terminal factors of the last
+ * implicit wds_forward (no new factorisation): row b of this call is
+ * right-hand side number first + b and uses the kept state of scenario
+ * (first + b) / rhs_per.  Arrays as in wds_adjoint with `batch` rows;
+ * batch <= the plan's max_batch (the rows' scratch), and every row must fall
+ * on a kept scenario.  Replaces the multi-column solve of
+ * sensitivity_matrix (dgga/sensitivity.py:59-145: one splu per frame, then
+ * lu.solve(V, trans='T') over m sensor columns). */
+int wds_adjoint_rhs(WdsPlan* plan, int32_t batch, int32_t rhs_per, int32_t first,
+                    const double* gH, const double* gQ, const double* gE, double* gd,
+                    double* grh, double* gke, double* gr, void* stream);
+
 /* Device arrays of one plan in a multi-plan call (shapes as in wds_forward /
  * wds_adjoint). */
 typedef struct WdsForwardIO {

@@ -17,6 +17,7 @@ and the reference outputs of
 
 Usage:  python tests/golden/make_golden.py        (steady cases)
         python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
+        python tests/golden/make_golden.py sens   (sensitivity-matrix pin, sens_ref.npz)
 """
 import json
 import os
@@ -220,8 +221,51 @@ def make_eps(T=6):
         frames["t_sec"].tolist(), frames["iterations"].tolist(), os.path.basename(path)))
 
 
+def make_sens():
+    """Sensitivity pin: the reference's sensitivity_matrix (dgga/sensitivity.py:
+    59-145, one splu per frame and m sensor columns, EPANET-replica mode) on
+    the config-2 network, two frames, six sensors, w.r.t. C and w.r.t. r."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    import dgga.sensitivity
+    torch.set_default_dtype(torch.float64)
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, 2, seed=61)
+    sens = synth.sensor_nodes(net, 6, seed=9)
+    ref_net = dgga.parse.Net(**net.as_fields())
+    # mode="epanet": the reference's polished solve runs the status machine
+    # there (its dense mode refuses PRV networks without it)
+    sd = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
+    r = np.asarray(net.r_hw, dtype=np.float64)
+    # device statuses of each frame from the reference's own batched status
+    # machine (sensitivity_matrix freezes the statuses it is given)
+    dn = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
+    st = dn.solve(torch.tensor(d), torch.tensor(rh), status_machine=True, accuracy=1e-10,
+                  assemble="csr", linear_solver="dense")["status"].numpy()
+    res = {"status": st}
+    for wrt in ("C", "r"):
+        blocks = []
+        for b in range(d.shape[0]):
+            S = dgga.sensitivity.sensitivity_matrix(
+                sd, torch.tensor(d[b:b + 1]), torch.tensor(rh[b:b + 1]), torch.tensor(r), sens,
+                wrt=wrt, accuracy=1e-10, status=st[b])
+            blocks.append(np.asarray(S))
+        res["S_" + wrt] = np.concatenate(blocks, axis=0)
+    blob = pack_net(net)
+    blob.update({"in_demand": d, "in_res_head": rh, "in_sensors": np.asarray(sens)})
+    blob.update({"ref_" + k: v for k, v in res.items()})
+    path = os.path.join(HERE, "sens_ref.npz")
+    np.savez_compressed(path, **blob)
+    print("sens: S_C %s, max |S_C| %.3g -> %s" % (res["S_C"].shape, np.abs(res["S_C"]).max(),
+                                                  os.path.basename(path)))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["eps"]:
         make_eps()
+    elif sys.argv[1:] == ["sens"]:
+        make_sens()
     else:
         main()

@@ -25,7 +25,7 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
            "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc",
-           "wds_forward_multi", "wds_adjoint_multi")
+           "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs")
 MULTI_MAX = 8
 
 
@@ -104,6 +104,9 @@ def load():
     lib.wds_adjoint_multi.argtypes = [ctypes.c_int32, ctypes.POINTER(vp), c_int32_p,
                                       ctypes.POINTER(WdsAdjointIO), vp]
     lib.wds_adjoint_multi.restype = ctypes.c_int
+    lib.wds_adjoint_rhs.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + \
+        [vp] * 7 + [vp]
+    lib.wds_adjoint_rhs.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]
     lib.wds_plan_stats.restype = ctypes.c_int
     lib.wds_plan_symbolic.argtypes = [vp] + [c_int32_p] * 5

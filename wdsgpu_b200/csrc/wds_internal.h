@@ -154,6 +154,11 @@ struct AdjArgs {
   double* grh;
   double* gke;
   double* gr;
+  // several right-hand sides per kept scenario: row b of this call (the
+  // (v0 + b)-th right-hand side) uses the kept state of scenario
+  // (v0 + b) / rhs_per; 0 or 1 means one right-hand side per scenario
+  int rhs_per = 1;
+  int v0 = 0;
 };
 
 // Host-side symbolic data kept in the plan (for inspection and tests).

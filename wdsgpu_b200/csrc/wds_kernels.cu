@@ -1424,23 +1424,26 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
     if (g >= groups || b >= a.B) return;
     s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   }
-  s.Mg = w.M + (size_t)b * n.nT * n.nT;  // terminal top-block inverse of the forward
-  if (!w.valid[b]) return;  // uniform per group
-  const FT* Wt = reinterpret_cast<const FT*>(w.W) + (size_t)b * n.nnzL;
+  // kept state of scenario bf (several right-hand sides per scenario read the
+  // same factor); right-hand sides, results and scratch are per b
+  const int bf = (a.v0 + b) / (a.rhs_per > 1 ? a.rhs_per : 1);
+  s.Mg = w.M + (size_t)bf * n.nT * n.nT;  // terminal top-block inverse of the forward
+  if (!w.valid[bf]) return;  // uniform per group
+  const FT* Wt = reinterpret_cast<const FT*>(w.W) + (size_t)bf * n.nnzL;
   for (int t = gtid<NT>(); t < n.nnzL; t += NT) wp<FT>(s)[t] = Wt[t];
-  for (int k = gtid<NT>(); k < n.L; k += NT) s.P[k] = w.P[(size_t)b * n.L + k];
+  for (int k = gtid<NT>(); k < n.L; k += NT) s.P[k] = w.P[(size_t)bf * n.L + k];
   const int pc = n.npcv > 0 ? n.npcv : 1;
   // status is only consulted for ACTIVE flags of PRVs
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     const int i = n.link_pcv[k];
-    s.S[k] = (i >= 0 && w.act[(size_t)b * pc + i]) ? WDS_ACTIVE : WDS_OPEN;
+    s.S[k] = (i >= 0 && w.act[(size_t)bf * pc + i]) ? WDS_ACTIVE : WDS_OPEN;
   }
   gsync<NT>();
   // emitter slots from the stored 1/hgrad (positive exactly at emitters)
-  build_emitters<NT>(n, s, w.emh + (size_t)b * n.Nj, 0);
+  build_emitters<NT>(n, s, w.emh + (size_t)bf * n.Nj, 0);
   for (int p = gtid<NT>(); p < n.Nj; p += NT) {
     const int es = s.eslot[p];
-    if (es >= 0) s.em_emh[es] = w.emh[(size_t)b * n.Nj + p];
+    if (es >= 0) s.em_emh[es] = w.emh[(size_t)bf * n.Nj + p];
   }
   gsync<NT>();
   const double* gH = a.gH + (size_t)b * n.N;
@@ -1539,8 +1542,8 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
   double* gke = a.gke + (size_t)b * n.N;
   double* grh = a.grh + (size_t)b * n.N;
   double* gr = a.gr + (size_t)b * n.L;
-  const double* hge = w.hge + (size_t)b * n.Nj;
-  const double* dke = w.dke + (size_t)b * n.Nj;
+  const double* hge = w.hge + (size_t)bf * n.Nj;
+  const double* dke = w.dke + (size_t)bf * n.Nj;
   for (int p = gtid<NT>(); p < n.Nj; p += NT) {
     const int nd = n.jnode[p];
     gd[nd] = lam[p];
@@ -1552,7 +1555,7 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
     gke[nd] = g;
     grh[nd] = 0.0;
   }
-  const double* dr = w.dr + (size_t)b * n.L;
+  const double* dr = w.dr + (size_t)bf * n.L;
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     const double l1 = junc_of(T.e1[k], lam), l2 = junc_of(T.e2[k], lam);
     const double lam_l = s.P[k] * (gQ[k] - (l2 - l1));

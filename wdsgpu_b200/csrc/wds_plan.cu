@@ -753,6 +753,29 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   return WDS_OK;
 }
 
+extern "C" int wds_adjoint_rhs(WdsPlan* plan, int32_t batch, int32_t rhs_per, int32_t first,
+                               const double* gH, const double* gQ, const double* gE,
+                               double* gd, double* grh, double* gke, double* gr,
+                               void* stream) {
+  using namespace wds;
+  if (!plan || batch <= 0 || rhs_per <= 0 || first < 0 || !gH || !gQ || !gE || !gd || !grh ||
+      !gke || !gr)
+    return fail(WDS_E_ARG, "wds_adjoint_rhs: bad argument");
+  if (batch > plan->max_batch)
+    return fail(WDS_E_ARG, "wds_adjoint_rhs: batch exceeds the plan's max_batch");
+  if (!plan->have_state)
+    return fail(WDS_E_STATE, "wds_adjoint_rhs: no implicit forward to differentiate");
+  if ((int64_t)first + batch - 1 >= (int64_t)plan->state_batch * rhs_per)
+    return fail(WDS_E_ARG, "wds_adjoint_rhs: rows beyond the kept scenarios");
+  AdjArgs a{batch, gH, gQ, gE, gd, grh, gke, gr};
+  a.rhs_per = rhs_per;
+  a.v0 = first;
+  std::string err;
+  int rc = launch_adjoint(plan->dn, plan->dw, a, plan->groups, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  return WDS_OK;
+}
+
 extern "C" int wds_forward_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batch,
                                  const WdsForwardOpts* opts, const WdsForwardIO* io,
                                  void* stream) {
