@@ -913,7 +913,11 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
       if (actf[i] != 0.0) rp[n.pcv_j2[i]] = -rprv[i];
   }
   gsync<NT>();
-  solve_refined<NT, FT>(n, T, s, rp, -1, dH, t, refine);
+  // The outer refinement below (two steps against the true M_p) contracts the
+  // error of this solve and of its own corrections by about kappa * u each, so
+  // these solves take no inner refinement; the fixed point is set by the FP64
+  // residual and does not depend on it.
+  solve_refined<NT, FT>(n, T, s, rp, -1, dH, t, 0);
   for (int c = 0; c < m; ++c) {
     // columns of inactive valves meet y = 0 in the correction: zero, not solved
     if (actf[c < p ? c : c - p] == 0.0) {
@@ -972,7 +976,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
         if (actf[i] != 0.0) res[n.pcv_j2[i]] = rp[n.pcv_j2[i]] - dH[n.pcv_j2[i]];
     }
     gsync<NT>();
-    solve_refined<NT, FT>(n, T, s, res, -1, sx, t, refine);
+    solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 0);
     wood(sx, res);
     for (int q = tid; q < n.Nj; q += NT) dH[q] = dH[q] + sx[q];
     gsync<NT>();
@@ -1490,7 +1494,8 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
       for (int i = 0; i < p; ++i)
         if (actf[i] != 0.0) r2[n.pcv_j2[i]] = gQ[n.pcv_link[i]];
     gsync<NT>();
-    solve_refined<NT, FT>(n, T, s, r2, -1, lam, t, 2);
+    // unrefined solves: the two outer refinement steps below contract their error
+    solve_refined<NT, FT>(n, T, s, r2, -1, lam, t, 0);
     for (int c = 0; c < p; ++c) {
       if (actf[c] == 0.0) {  // meets y = 0 in the correction
         for (int q = gtid<NT>(); q < n.Nj; q += NT) cols[(size_t)c * n.Nj + q] = 0.0;
@@ -1531,7 +1536,7 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
           if (actf[i] != 0.0)
             res[n.pcv_j2[i]] = r2[n.pcv_j2[i]] - (lam[n.pcv_j2[i]] - lam[n.pcv_j1[i]]);
       gsync<NT>();
-      solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 2);
+      solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 0);
       wood(sx, res);
       for (int q = gtid<NT>(); q < n.Nj; q += NT) lam[q] = lam[q] + sx[q];
       gsync<NT>();
