@@ -117,6 +117,9 @@ typedef struct WdsNetwork {
                                     solve refined against the FP64 operator (the
                                     precision choice dense_refine / cudss_refine leave
                                     open, dgga/solver.py:182, 384); 0: FP64 */
+  const double* pump_hunit;      /* [L] pumpstatus shut-off head at unit speed (BIG for
+                                    constant-HP pumps), used when a call passes its own
+                                    pump speeds; NULL: pump_hmax / pump_speed^2 */
 } WdsNetwork;
 
 /* WdsNetwork.layout */
@@ -139,6 +142,14 @@ typedef struct WdsForwardOpts {
    * emitter flow 1 where Ke > 0). */
   const double* q0;              /* [B,L] initial link flows, or NULL        */
   const double* e0;              /* [B,N] initial emitter flows (read at junctions with Ke > 0), or NULL */
+  /* Pump parameters of this call (the speed / pump_h0 / pump_r of
+   * implicit_solve, dgga/autodiff.py:1315-1342): rows of [L] values read at
+   * pump links, one row for all scenarios (pump_stride 0) or one per
+   * scenario (pump_stride L); NULL: the network's own. */
+  const double* pump_speed;      /* relative speed (link setting)           */
+  const double* pump_h0;         /* curve coefficient H0                    */
+  const double* pump_r;          /* curve coefficient R                     */
+  int64_t pump_stride;
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;
@@ -169,6 +180,18 @@ int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* opts,
 int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH,
                 const double* gQ, const double* gE, double* gd, double* grh,
                 double* gke, double* gr, void* stream);
+
+/* wds_adjoint plus the pump-parameter gradients [B,L] (zero off pump links):
+ * gspeed = dLoss/d(relative speed), gh0 = dLoss/d(curve H0), grp =
+ * dLoss/d(curve R), per scenario, at the speeds / coefficients the forward
+ * was given in WdsForwardOpts (or the network's own).  Replaces the pump
+ * theta of the CPU adjoint ImplicitGGASolve.backward
+ * (dgga/autodiff.py:660-756, coefficients from _pump_coeffs_np :122-218),
+ * which sums these rows over the batch for [L] parameters. */
+int wds_adjoint_pumps(WdsPlan* plan, int32_t batch, const double* gH,
+                      const double* gQ, const double* gE, double* gd, double* grh,
+                      double* gke, double* gr, double* gspeed, double* gh0, double* grp,
+                      void* stream);
 
 /* Statistics of the plan: [Nj, nnz_L, n_levels, n_pairs, smem_bytes,
  * n_pcv, nnz_A_lower, threads]. */

@@ -21,6 +21,8 @@ by the reference itself (tests/golden/*.npz, see tests/test_oracle_golden.py).
 """
 from __future__ import annotations
 
+import copy
+
 import numpy as np
 import scipy.linalg as sla
 
@@ -284,6 +286,71 @@ class Model:
         P = np.where(self.p_nocurve, 1.0 / CSMALL, P)
         Y = np.where(self.p_nocurve, q, Y)
         return P, Y
+
+    def with_pumps(self, speed=None, h0=None, r=None):
+        """A copy of the model at a call's pump parameters ([L] rows, read at
+        pump links): the speed / pump_h0 / pump_r of implicit_solve
+        (autodiff.py:99-120 _resolve_pump_args).  Speed also sets the
+        zero-speed closed branch and the pumpstatus shut-off head
+        (solver.py:665-679)."""
+        m = copy.copy(self)
+        if speed is not None:
+            sp = np.where(self.is_pump, np.asarray(speed, dtype=np.float64), self.speed)
+            m.speed = sp
+            m.zero_speed = self.is_pump & (sp == 0.0)
+            m.pump_live = self.is_pump & (sp > 0.0)
+            m.pump_hmax_sm = np.where(self.p_chp, BIG, sp * sp * self.p_hmax)
+            m.closed_dense = self.closed0 | m.zero_speed
+        if h0 is not None:
+            m.p_h0 = np.where(self.is_pump, np.asarray(h0, dtype=np.float64), self.p_h0)
+        if r is not None:
+            m.p_r = np.where(self.is_pump, np.asarray(r, dtype=np.float64), self.p_r)
+        return m
+
+    def pump_dtheta(self, q, S):
+        """d hloss / d(speed, H0, R) of every pump at flows q [B,L] with the
+        statuses S frozen (autodiff.py:122-218 _pump_coeffs_np,
+        hydcoeffs.c:673-791); three [B,L] arrays, zero off pumps and on the
+        closed / zero-speed / NOCURVE / clamped constant-HP branches."""
+        B = q.shape[0]
+        dw, dh0, dR = np.zeros((B, self.L)), np.zeros((B, self.L)), np.zeros((B, self.L))
+        for k in np.flatnonzero(self.is_pump):
+            w = float(self.speed[k])
+            t = int(self.p_type[k])
+            for b in range(B):
+                if S is not None and S[b, k] <= CLOSED or w == 0.0 or t == 3:
+                    continue
+                qk = float(q[b, k])
+                qa = abs(qk)
+                if t == 2:   # frozen curve segment: hloss = w^2 H0c + w Rc q
+                    cx, cy = self.curves[int(k)]
+                    qq = (qa / w) * self.ucf_flow
+                    i2 = min(max(int(np.searchsorted(cx, qq, side="left")), 1), cx.size - 1)
+                    i1 = i2 - 1
+                    rc = (cy[i2] - cy[i1]) / (cx[i2] - cx[i1])
+                    h0c = (cy[i1] - rc * cx[i1]) / self.ucf_head
+                    rc = rc * self.ucf_flow / self.ucf_head
+                    dw[b, k] = 2.0 * w * (-h0c) + (-rc) * qk
+                    continue
+                n, H0, R = float(self.p_n[k]), float(self.p_h0[k]), float(self.p_r[k])
+                if t == 0:   # constant HP: hloss = r / q, r = R w^(2-n)
+                    hgr = -(R * w ** (2.0 - n)) / qa / qa if qa > 0.0 else np.inf
+                    if self.rqtol <= hgr <= CBIG:
+                        dw[b, k] = (2.0 - n) * R * w ** (1.0 - n) / qk
+                        dR[b, k] = w ** (2.0 - n) / qk
+                    continue
+                dh0[b, k] = w * w
+                if n == 1.0:  # linear curve: hloss = w^2 H0 + R w q
+                    dw[b, k] = 2.0 * w * H0 + R * qk
+                    dR[b, k] = w * qk
+                    continue
+                pw = qa ** (n - 1.0) if qa > 0.0 else (0.0 if n > 1.0 else np.inf)
+                if n * (R * w ** (2.0 - n)) * pw < self.rqtol:   # RQtol clamp
+                    dw[b, k] = 2.0 * w * H0
+                    continue
+                dw[b, k] = 2.0 * w * H0 + (2.0 - n) * R * w ** (1.0 - n) * pw * qk
+                dR[b, k] = w ** (2.0 - n) * pw * qk
+        return dw, dh0, dR
 
     def emitter(self, e, ke):
         """Emitter head loss and gradient (solver.py:2368-2377)."""
@@ -724,8 +791,9 @@ class Model:
             lam = lam + wood(self._solveA(kf, P, emh, act, res), res)
         return lam
 
-    def adjoint(self, q, e, ke, r, S, kf, gH, gQ, gE):
-        """Reduced adjoint (autodiff.py:1246-1312); gradients stay [B,*]."""
+    def adjoint(self, q, e, ke, r, S, kf, gH, gQ, gE, pumps=False):
+        """Reduced adjoint (autodiff.py:1246-1312); gradients stay [B,*].
+        pumps: also the pump-theta gradients (d speed, d H0, d R) [B,L]."""
         B = q.shape[0]
         P, _, emh, hge, em, dr, dke, act = self.adj_coeffs(q, e, ke, r, S)
         gHj, gEj = gH[:, self.junc], gE[:, self.junc]
@@ -748,6 +816,8 @@ class Model:
             np.add.at(grh[b], self.f2_nodes, -lam_l[b, self.lk_f2])
         grh = grh + gH * self.fixmask
         gr = -(lam_l * dr)
+        if pumps:   # pump theta: -lam_l d hloss / d theta (autodiff.py:736-741)
+            return (gd, grh, gke, gr) + tuple(-(lam_l * x) for x in self.pump_dtheta(q, S))
         return gd, grh, gke, gr
 
     def implicit(self, d, rh, ke=None, r=None, accuracy=1e-12, max_iter=200,
@@ -776,6 +846,6 @@ class Model:
         return dict(head_ft=H, flow_cfs=q, emitter_cfs=emit, iters=out["iters"],
                     status=S), state
 
-    def backward(self, state, gH, gQ, gE):
+    def backward(self, state, gH, gQ, gE, pumps=False):
         return self.adjoint(state["q"], state["e"], state["ke"], state["r"],
-                            state["S"], state["kf"], gH, gQ, gE)
+                            state["S"], state["kf"], gH, gQ, gE, pumps=pumps)

@@ -18,6 +18,7 @@ and the reference outputs of
 Usage:  python tests/golden/make_golden.py        (steady cases)
         python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
         python tests/golden/make_golden.py sens   (sensitivity-matrix pin, sens_ref.npz)
+        python tests/golden/make_golden.py pumps  (pump-parameter gradient pin, pump_ref.npz)
 """
 import json
 import os
@@ -262,10 +263,71 @@ def make_sens():
                                                   os.path.basename(path)))
 
 
+def make_pumps():
+    """Pump-parameter pin: the reference's CPU implicit adjoint with pump theta
+    (ImplicitGGASolve, dgga/autodiff.py:609-756: speed / pump_h0 / pump_r as
+    differentiable [L] tensors, statuses frozen) on the feature network with
+    all four pump kinds (power function, custom curve, no curve, constant HP),
+    at speeds and curve coefficients moved off the network's values.  One
+    scenario per call (the statuses are per scenario); the loss is the sum of
+    squared heads at the sensors and at the pumps' downstream nodes plus the
+    sum of squared pump flows."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.feature_network(tank_level=0.5, with_chp=True)
+    d, _ = synth.config2_scenarios(net, 3, seed=17, sigma=0.3)
+    rh = np.broadcast_to(net.fixed_head_ft_at(0), d.shape).copy()
+    ke = np.asarray(net.node_ke, dtype=np.float64)
+    sens = synth.sensor_nodes(net, 6)
+    ref_net = dgga.parse.Net(**net.as_fields())
+    se = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
+    pl = np.asarray(net.pump_link, dtype=np.int64)
+    pn2 = np.asarray(net.link_n2, dtype=np.int64)[pl]
+    speed = np.asarray(se.init_setting, dtype=np.float64).copy()
+    speed[pl] = speed[pl] * np.array([0.97, 1.04, 1.0, 1.02])
+    h0 = np.asarray(se.pl_h0, dtype=np.float64).copy()
+    h0[pl[0]] *= 1.03
+    rp = np.asarray(se.pl_r, dtype=np.float64).copy()
+    rp[pl[0]] *= 0.95
+    rp[pl[3]] *= 1.05
+    dn = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
+    st = dn.solve(torch.tensor(d), torch.tensor(rh), status_machine=True, accuracy=1e-10,
+                  assemble="csr", linear_solver="dense")["status"].numpy()
+    keys = ("head", "flow", "g_speed", "g_h0", "g_r", "g_demand", "g_rhw")
+    res = {k: [] for k in keys}
+    for b in range(d.shape[0]):
+        D = torch.tensor(d[b:b + 1]).requires_grad_(True)
+        R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+        sp = torch.tensor(speed).requires_grad_(True)
+        h0t = torch.tensor(h0).requires_grad_(True)
+        rpt = torch.tensor(rp).requires_grad_(True)
+        h, q, e = dgga.autodiff.implicit_solve(
+            se, D, torch.tensor(rh[b:b + 1]), ke=torch.tensor(ke), r_hw=R, accuracy=1e-10,
+            adjoint="cpu", speed=sp, pump_h0=h0t, pump_r=rpt, status=st[b])
+        loss = (h[:, sens] ** 2).sum() + (h[:, pn2] ** 2).sum() + (q[:, pl] ** 2).sum()
+        loss.backward()
+        for k, v in zip(keys, (h.detach(), q.detach(), sp.grad, h0t.grad, rpt.grad, D.grad,
+                               R.grad)):
+            res[k].append(np.asarray(v).reshape(-1))
+    blob = pack_net(net)
+    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
+                 "in_speed": speed, "in_pump_h0": h0, "in_pump_r": rp, "in_status": st})
+    blob.update({"ref_" + k: np.stack(v) for k, v in res.items()})
+    path = os.path.join(HERE, "pump_ref.npz")
+    np.savez_compressed(path, **blob)
+    print("pumps: g_speed at pumps %s -> %s" % (
+        np.stack(res["g_speed"])[:, pl].tolist(), os.path.basename(path)))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["eps"]:
         make_eps()
     elif sys.argv[1:] == ["sens"]:
         make_sens()
+    elif sys.argv[1:] == ["pumps"]:
+        make_pumps()
     else:
         main()

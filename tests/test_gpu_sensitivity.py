@@ -51,3 +51,24 @@ def test_sensitivity_rows_in_several_launches(cuda):
     S = sensitivity_matrix(s, d, rh, None, sens, wrt="r", accuracy=1e-7)
     R = oracle_sensitivity(net, d, rh, sens, "r", accuracy=1e-7)
     assert np.abs(S - R).max() <= 1e-6 * np.abs(R).max()
+
+
+def test_sensitivity_at_call_pump_speeds(cuda):
+    """speed / pump_h0 / pump_r of the call set the frames' pumps (the
+    reference's sensitivity_matrix takes them likewise)."""
+    from wdsgpu_b200.sensitivity import sensitivity_matrix
+    from wdsgpu_b200.solver import GGASolver
+    from test_sensitivity_oracle import oracle_sensitivity   # puts the repo root on sys.path
+    from oracle.gga import Model
+    net, inp, _ = load("pump_ref")
+    s = GGASolver(net, device=cuda, dense_status_machine=True)
+    S = sensitivity_matrix(s, inp["demand"], inp["res_head"], None, inp["sensors"], wrt="r",
+                           accuracy=1e-7, speed=inp["speed"], pump_h0=inp["pump_h0"],
+                           pump_r=inp["pump_r"])
+    m = Model(net).with_pumps(inp["speed"], inp["pump_h0"], inp["pump_r"])
+    R = oracle_sensitivity(net, inp["demand"], inp["res_head"], inp["sensors"], "r",
+                           accuracy=1e-7, model=m)
+    assert np.abs(S - R).max() <= 1e-8 * np.abs(R).max()
+    S0 = sensitivity_matrix(s, inp["demand"], inp["res_head"], None, inp["sensors"], wrt="r",
+                            accuracy=1e-7)
+    assert np.abs(S - S0).max() > 1e-6 * np.abs(R).max()     # the speeds matter

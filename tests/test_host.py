@@ -73,7 +73,7 @@ def test_implicit_solve_guards():
         implicit_solve(s, d, rh, adjoint="cpu")
     with pytest.raises(ValueError):
         implicit_solve(s, d, rh, adjoint="both")
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):                 # pump rows are [L] or [B, L]
         implicit_solve(s, d, rh, speed=np.ones(3))
 
 
@@ -113,3 +113,28 @@ def test_synthetic_networks_are_seeded():
     assert (np.asarray(a.link_type) == 3).sum() == 3
     assert (np.asarray(a.link_type) == 1).sum() == 905
     assert (a.node_ke > 0).sum() == 20
+
+
+def test_pump_rows_host_rules():
+    """speed / pump_h0 / pump_r rows: [L] or [B,L]; speed equals the
+    network's link settings off pump links (the reference's speed sets valve
+    settings there, dgga/autodiff.py:99-120)."""
+    net = synth.feature_network(with_chp=True)
+    s = GGASolver(net, device="cpu", dense_status_machine=True)
+    pl = np.asarray(net.pump_link)
+    sp = s.init_setting.copy()
+    sp[pl] *= 1.05
+    rows = s.pump_rows(3, speed=sp)
+    assert rows[0].shape == (1, s.L) and rows[1] is None and rows[2] is None
+    rows = s.pump_rows(3, speed=sp, pump_h0=np.tile(np.zeros(s.L), (3, 1)))
+    assert rows[0].shape == (3, s.L) and rows[1].shape == (3, s.L)
+    assert s.pump_rows(3) is None
+    with pytest.raises(ValueError):
+        s.pump_rows(3, pump_r=np.zeros((2, s.L)))
+    bad = sp.copy()
+    bad[np.flatnonzero(np.asarray(net.link_type) != 2)[0]] += 1.0   # a non-pump link
+    with pytest.raises(NotImplementedError):
+        s.pump_rows(3, speed=bad)
+    with pytest.raises(NotImplementedError):                         # frozen status
+        implicit_solve(s, net.demand_cfs_at(0), net.fixed_head_ft_at(0),
+                       status=np.zeros(s.L, dtype=np.int8))

@@ -14,10 +14,10 @@ from golden.load import load  # noqa: E402
 from oracle.gga import Model  # noqa: E402
 
 
-def oracle_sensitivity(net, d, rh, sensors, wrt, accuracy=1e-10):
+def oracle_sensitivity(net, d, rh, sensors, wrt, accuracy=1e-10, model=None):
     """S[B*m, L]: one batched adjoint per sensor (unit right-hand side at that
     sensor in every frame), rows frame-major."""
-    m = Model(net)
+    m = Model(net) if model is None else model
     out, st = m.implicit(d, rh, accuracy=accuracy)
     B, ms = d.shape[0], len(sensors)
     S = np.empty((B, ms, net.L))

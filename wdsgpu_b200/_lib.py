@@ -25,7 +25,7 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
            "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc",
-           "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs")
+           "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs", "wds_adjoint_pumps")
 MULTI_MAX = 8
 
 
@@ -53,6 +53,7 @@ class WdsNetwork(ctypes.Structure):
         ("perm", c_int32_p),
         ("emitter_capacity", ctypes.c_int32),
         ("layout", ctypes.c_int32), ("factor_fp32", ctypes.c_int32),
+        ("pump_hunit", c_double_p),
     ]
 
 
@@ -62,6 +63,8 @@ class WdsForwardOpts(ctypes.Structure):
         ("status_machine", ctypes.c_int32), ("refine", ctypes.c_int32),
         ("polish_steps", ctypes.c_int32), ("ke_stride", ctypes.c_int64),
         ("r_stride", ctypes.c_int64), ("q0", ctypes.c_void_p), ("e0", ctypes.c_void_p),
+        ("pump_speed", ctypes.c_void_p), ("pump_h0", ctypes.c_void_p),
+        ("pump_r", ctypes.c_void_p), ("pump_stride", ctypes.c_int64),
     ]
 
 
@@ -107,6 +110,8 @@ def load():
     lib.wds_adjoint_rhs.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + \
         [vp] * 7 + [vp]
     lib.wds_adjoint_rhs.restype = ctypes.c_int
+    lib.wds_adjoint_pumps.argtypes = [vp, ctypes.c_int32] + [vp] * 10 + [vp]
+    lib.wds_adjoint_pumps.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]
     lib.wds_plan_stats.restype = ctypes.c_int
     lib.wds_plan_symbolic.argtypes = [vp] + [c_int32_p] * 5

@@ -12,8 +12,13 @@
   dL/d(demand, reservoir head, emitter Ke, pipe resistance).  1-D parameters
   receive the batch-summed gradient (dgga/autodiff.py:1306-1308).
 
+Pump parameters (speed, pump_h0, pump_r) are differentiable here too: the
+forward keeps d hloss / d theta of every pump at the terminal state and
+`wds_adjoint_pumps` contracts it with the link adjoint, the formulas of the
+reference's CPU adjoint (dgga/autodiff.py:122-218, 736-741).
+
 Refusals follow the reference: unconverged scenarios, second derivatives,
-pump parameters, constant-HP pumps on their clamp branch, PRVs that share a
+a frozen `status`, constant-HP pumps on their clamp branch, PRVs that share a
 downstream junction or cascade.
 """
 from __future__ import annotations
@@ -29,7 +34,9 @@ from .solver import CBIG, GGASolver, _not_pd_hint
 __all__ = ["implicit_solve", "ImplicitGGASolveSM100", "hw_resistance", "dr_dC"]
 
 
-def _adjoint_guards(s: GGASolver, flow, S):
+def _adjoint_guards(s: GGASolver, flow, S, pumps=None):
+    """Refusals of the reduced adjoint (dgga/autodiff.py:1157-1170); pumps is
+    the call's (speed, h0, r) rows of GGASolver.pump_rows, or None."""
     if s.n_pcv:
         j1 = s._n1[s.pcv_links]
         j2 = s._n2[s.pcv_links]
@@ -49,12 +56,14 @@ def _adjoint_guards(s: GGASolver, flow, S):
         q = flow.index_select(1, kt)
         sgn = torch.where(q < 0, -1.0, 1.0)
         qa = (q * sgn).clamp_min(1e-30)
-        sp = torch.as_tensor(np.maximum(t["pump_speed"][ks], 1e-12), device=dev)
-        re = torch.as_tensor(t["pump_r"][ks], device=dev) * sp ** (
-            2.0 - torch.as_tensor(t["pump_n"][ks], device=dev))
+        sp_row = (pumps[0].index_select(1, kt) if pumps is not None and pumps[0] is not None
+                  else torch.as_tensor(t["pump_speed"][ks], device=dev))
+        r_row = (pumps[2].index_select(1, kt) if pumps is not None and pumps[2] is not None
+                 else torch.as_tensor(t["pump_r"][ks], device=dev))
+        sp = sp_row.clamp_min(1e-12)
+        re = r_row * sp ** (2.0 - torch.as_tensor(t["pump_n"][ks], device=dev))
         raw = -re / qa / qa
-        closed = (S.index_select(1, kt) <= 2) | torch.as_tensor(
-            (t["flags"][ks] & _lib.F_ZERO_SPEED) != 0, device=dev)
+        closed = (S.index_select(1, kt) <= 2) | (sp_row == 0.0)
         bad = ~closed & ((raw > CBIG) | (raw < s.rqtol))
         if bool(bad.any()):
             raise NotImplementedError(
@@ -64,11 +73,15 @@ def _adjoint_guards(s: GGASolver, flow, S):
 
 class ImplicitGGASolveSM100(torch.autograd.Function):
     """(demand, res_head, ke, r_hw, solver, accuracy, max_iter, status_machine,
-    polish_steps) -> (head[B,N], flow[B,L], emitter[B,N])."""
+    polish_steps[, speed, pump_h0, pump_r]) -> (head[B,N], flow[B,L],
+    emitter[B,N]).  speed / pump_h0 / pump_r ([L] shared by the batch, or
+    [B,L]) are differentiable like the CPU adjoint's pump theta
+    (dgga/autodiff.py:609-756); an [L] parameter receives the batch sum."""
 
     @staticmethod
     def forward(ctx, demand, res_head, ke, r_hw, solver, accuracy=1e-12,
-                max_iter=200, status_machine=None, polish_steps=3):
+                max_iter=200, status_machine=None, polish_steps=3, speed=None,
+                pump_h0=None, pump_r=None):
         s = solver
         dims = (demand.dim(), res_head.dim(), ke.dim(), r_hw.dim())
         devs = (demand.device, res_head.device, ke.device, r_hw.device)
@@ -78,7 +91,10 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
                                            ke.detach(), r_hw.detach())
         if ke_t.shape[0] == 1 and B > 1:
             ke_t = ke_t.contiguous()
-        o = s.run(d, rh, ke_t, r_t, B, int(max_iter), float(accuracy), sm, int(polish_steps))
+        th_in = (speed, pump_h0, pump_r)
+        pumps = s.pump_rows(B, *th_in)
+        o = s.run(d, rh, ke_t, r_t, B, int(max_iter), float(accuracy), sm, int(polish_steps),
+                  pumps=pumps)
         info = o["info"]
         from .solver import _check_emitter_cap
         _check_emitter_cap(s, info)
@@ -92,8 +108,10 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
             raise RuntimeError(
                 "adjoint='gpu': scenarios %s did not converge (relerr=%s > accuracy=%g)"
                 % (bad[:8], [float(o["relerr"][b]) for b in bad[:4]], float(accuracy)))
-        _adjoint_guards(s, o["flow"], o["status"])
+        _adjoint_guards(s, o["flow"], o["status"], pumps)
         ctx.solver = s
+        ctx.pumps = pumps      # keeps the rows alive with the kept state
+        ctx.th = tuple(None if x is None else (x.dim(), x.device) for x in th_in)
         ctx.plan = o["plan"]
         ctx.B = B
         ctx.dims = dims
@@ -129,10 +147,19 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         p = ctx.plan
         cur = torch.cuda.current_stream(dev)
         ev = s._event_pair(cur, "adjoint")
-        _lib.check(p.lib.wds_adjoint(
-            p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
-            grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
-            "wds_adjoint")
+        want_th = any(x is not None for x in ctx.th) and any(ctx.needs_input_grad[9:12])
+        if want_th:
+            gth = torch.empty(3, B, L, dtype=torch.float64, device=dev)
+            _lib.check(p.lib.wds_adjoint_pumps(
+                p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
+                grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), gth[0].data_ptr(),
+                gth[1].data_ptr(), gth[2].data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
+                "wds_adjoint_pumps")
+        else:
+            _lib.check(p.lib.wds_adjoint(
+                p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
+                grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
+                "wds_adjoint")
         if ev is not None:
             ev[1].record(cur)
         dm, dv = ctx.dims, ctx.devs
@@ -141,8 +168,13 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
             g = g.to(device=d_)
             return g.sum(0) if dim == 1 else g
 
+        g_th = [None, None, None]
+        if want_th:
+            for i, meta in enumerate(ctx.th):
+                if meta is not None and ctx.needs_input_grad[9 + i]:
+                    g_th[i] = _fit(gth[i], meta[0], meta[1])
         return (_fit(gd, dm[0], dv[0]), _fit(grh, dm[1], dv[1]), _fit(gke, dm[2], dv[2]),
-                _fit(gr, dm[3] + 1, dv[3]), None, None, None, None, None)
+                _fit(gr, dm[3] + 1, dv[3]), None, None, None, None, None, *g_th)
 
 
 def implicit_solve(solver, demand, res_head, ke=None, r_hw=None, accuracy=1e-12,
@@ -150,18 +182,21 @@ def implicit_solve(solver, demand, res_head, ke=None, r_hw=None, accuracy=1e-12,
                    status=None, adjoint="gpu", status_machine=None, assemble="csr",
                    linear_solver="sm100"):
     """Forward + implicit adjoint (dgga/autodiff.py:1315-1351 contract).
-    Returns (head, flow, emitter); differentiable w.r.t. demand, res_head, ke
-    and r_hw."""
+    Returns (head, flow, emitter); differentiable w.r.t. demand, res_head, ke,
+    r_hw and the pump parameters speed / pump_h0 / pump_r ([L] or [B,L]; the
+    reference takes these on its CPU adjoint only, dgga/autodiff.py:609-756).
+    status (a frozen internal status) is refused: the batched status machine
+    decides each scenario's status."""
     if adjoint == "cpu":
         raise NotImplementedError(
             "adjoint='cpu' is the reference's scipy splu adjoint; this package "
             "provides adjoint='gpu'")
     if adjoint != "gpu":
         raise ValueError("adjoint must be 'cpu'/'gpu', got %r" % (adjoint,))
-    if speed is not None or pump_h0 is not None or pump_r is not None or status is not None:
+    if status is not None:
         raise NotImplementedError(
-            "adjoint='gpu' takes no speed/pump_h0/pump_r/status (pump parameter "
-            "gradients are CPU-adjoint only in the reference)")
+            "adjoint='gpu' takes no status: the batched status machine decides "
+            "each scenario's status")
     if assemble != "csr" or linear_solver != "sm100":
         raise ValueError("the B200 route is assemble='csr', linear_solver='sm100'")
     dev = solver.device
@@ -169,8 +204,10 @@ def implicit_solve(solver, demand, res_head, ke=None, r_hw=None, accuracy=1e-12,
         else torch.as_tensor(np.asarray(x), dtype=torch.float64, device=dev)
     ke = solver.node_ke_default if ke is None else ke
     r_hw = solver.r_hw if r_hw is None else r_hw
+    tn = lambda x: None if x is None else t(x)
     return ImplicitGGASolveSM100.apply(t(demand), t(res_head), t(ke), t(r_hw), solver,
-                                       accuracy, max_iter, status_machine, int(polish_steps))
+                                       accuracy, max_iter, status_machine, int(polish_steps),
+                                       tn(speed), tn(pump_h0), tn(pump_r))
 
 
 # Roughness chain rule (dgga/calib.py:64-89): r = 4.727 L / C^1.852 / D^4.871.

@@ -37,6 +37,9 @@ struct DevNet {
   const double* pn;
   const double* pspeed;
   const double* phmax;
+  const double* phunit;   // [L] shut-off head at unit speed (pumpstatus)
+  const int* link_pump;   // [L] pump index or -1
+  int npump;
   const int* cptr;        // [L+1]
   const double* cx;
   const double* cy;
@@ -121,6 +124,7 @@ struct DevWork {
   double* lk;     // [B][2][L] link flows q and Y of the forward
   double* M;      // [B][nT][nT] inverse of the top block's Schur complement
   unsigned char* state;  // [B][state bytes] scenario state of large networks (else null)
+  double* dpump;  // [B][3][npump] dhloss/d(speed, H0, R) of each pump at the terminal state
   int nscr;
   int* valid;     // [B] 1 when the terminal state is stored
 };
@@ -136,6 +140,11 @@ struct FwdArgs {
   const double* r;
   const double* q0;  // [B][L] warm-start flows or null
   const double* e0;  // [B][N] warm-start emitter flows or null
+  // pump parameters of the call ([L] rows, stride 0 or L; null: the network's)
+  const double* th_sp;
+  const double* th_h0;
+  const double* th_r;
+  long long th_stride;
   double* head;
   double* flow;
   double* emit;
@@ -154,6 +163,10 @@ struct AdjArgs {
   double* grh;
   double* gke;
   double* gr;
+  // pump-parameter gradients [B][L] (null: not wanted)
+  double* gsp = nullptr;
+  double* gh0 = nullptr;
+  double* grp = nullptr;
   // several right-hand sides per kept scenario: row b of this call (the
   // (v0 + b)-th right-hand side) uses the kept state of scenario
   // (v0 + b) / rhs_per; 0 or 1 means one right-hand side per scenario

@@ -229,8 +229,36 @@ __device__ __forceinline__ void pipe_coef(const DevNet& n, double q, double r, d
   Y = hl / hg;
 }
 
+// Pump parameters of one scenario: rows of [L] values read at pump links
+// (the network's own, or the call's speed / pump_h0 / pump_r of
+// implicit_solve, dgga/autodiff.py:1315-1342), read through the kernel
+// arguments only where a pump needs them.  own_sp: the speeds are the call's,
+// so the zero-speed and pumpstatus tests are taken from them instead of the
+// network's link flags.
+struct PumpTh {
+  const FwdArgs& a;
+  const DevNet& n;
+  long long o;  // row offset of this scenario
+  __device__ __forceinline__ bool own_sp() const { return a.th_sp != nullptr; }
+  __device__ __forceinline__ double sp(int k) const { return a.th_sp ? a.th_sp[o + k] : n.pspeed[k]; }
+  __device__ __forceinline__ double h0(int k) const { return a.th_h0 ? a.th_h0[o + k] : n.ph0[k]; }
+  __device__ __forceinline__ double r(int k) const { return a.th_r ? a.th_r[o + k] : n.pr[k]; }
+};
+
+__device__ __forceinline__ PumpTh pump_th(const DevNet& n, const FwdArgs& a, int b) {
+  return PumpTh{a, n, (long long)b * a.th_stride};
+}
+
+// A pump on the closed branch for its speed alone (hydcoeffs.c:696-701 via
+// dgga/solver.py:673: setting == 0).
+__device__ __forceinline__ bool zero_speed(const DevNet& n, const PumpTh& th, int k, int kd) {
+  return th.own_sp() ? (kd == WDS_KIND_PUMP && th.sp(k) == 0.0)
+                     : (n.flags[k] & WDS_F_ZERO_SPEED) != 0;
+}
+
 // pumpcoeff for every curve kind (dgga/solver.py:2221-2326)
-__device__ void pump_coef(const DevNet& n, int k, double q, double& P, double& Y) {
+__device__ void pump_coef(const DevNet& n, const PumpTh& th, int k, double q, double& P,
+                          double& Y) {
   const int t = n.ptype[k];
   if (t == 3) {  // NOCURVE: an open valve
     P = 1.0 / kCSMALL;
@@ -239,7 +267,7 @@ __device__ void pump_coef(const DevNet& n, int k, double q, double& P, double& Y
   }
   const double sgn = q < 0.0 ? -1.0 : 1.0;
   const double qa = q * sgn;
-  const double spc = fmax(n.pspeed[k], 1e-12);
+  const double spc = fmax(th.sp(k), 1e-12);
   double hg, hl;
   if (t == 2) {  // CUSTOM: piecewise-linear curve segment
     const int c0 = n.cptr[k], np = n.cptr[k + 1] - c0;
@@ -257,8 +285,8 @@ __device__ void pump_coef(const DevNet& n, int k, double q, double& P, double& Y
     hl = (-h0c) * (spc * spc) + hg * q;
   } else {
     const double pn = n.pn[k];
-    const double h0e = spc * spc * n.ph0[k];
-    const double re = n.pr[k] * pow(spc, 2.0 - pn);
+    const double h0e = spc * spc * th.h0(k);
+    const double re = th.r(k) * pow(spc, 2.0 - pn);
     if (t == 0) {  // CONST_HP
       const double qac = fmax(qa, 1e-30);
       const double raw = -re / qac / qac;
@@ -310,8 +338,8 @@ __device__ __forceinline__ void prv_open(const DevNet& n, int i, double qk, int 
 // Link coefficients of the headloss stage (dgga/solver.py:2923-2956).
 // `adj` selects the adjoint/polish variant in which a status-machine PRV
 // takes its valve coefficients directly (autodiff.py:838-847).
-__device__ __forceinline__ void link_coef(const DevNet& n, int k, double q, int s, double r,
-                                          bool adj, double& P, double& Y) {
+__device__ __forceinline__ void link_coef(const DevNet& n, const PumpTh& th, int k, double q,
+                                          int s, double r, bool adj, double& P, double& Y) {
   const int kd = n.kind[k];
   if (kd == WDS_KIND_PRV) {
     if (!adj) {
@@ -325,7 +353,7 @@ __device__ __forceinline__ void link_coef(const DevNet& n, int k, double q, int 
     }
     return;
   }
-  if (s <= WDS_CLOSED || (n.flags[k] & WDS_F_ZERO_SPEED)) {
+  if (s <= WDS_CLOSED || zero_speed(n, th, k, kd)) {
     P = 1.0 / kCBIG;
     Y = q;
     return;
@@ -337,7 +365,60 @@ __device__ __forceinline__ void link_coef(const DevNet& n, int k, double q, int 
   else if (kd == WDS_KIND_PRV_FIXED)
     valve_open(n, q, n.km[k], P, Y);
   else
-    pump_coef(n, k, q, P, Y);
+    pump_coef(n, th, k, q, P, Y);
+}
+
+// d hloss / d(speed, H0, R) of one open pump at flow q with the curve
+// segment / clamp branch frozen (dgga/autodiff.py:122-218, the CPU adjoint's
+// pump theta; hydcoeffs.c:673-791).  Zero on the closed, zero-speed, NOCURVE
+// and clamped constant-HP branches.
+__device__ void pump_dtheta(const DevNet& n, const PumpTh& th, int k, double q, int st,
+                            double& dw, double& dh0, double& dR) {
+  dw = dh0 = dR = 0.0;
+  const double w = th.sp(k);
+  const int t = n.ptype[k];
+  if (st <= WDS_CLOSED || w == 0.0 || t == 3) return;
+  const double qa = fabs(q);
+  if (t == 2) {  // CUSTOM: dw = 2 w H0c + Rc q on the frozen segment
+    const int c0 = n.cptr[k], np = n.cptr[k + 1] - c0;
+    const double* X = n.cx + c0;
+    const double* Yc = n.cy + c0;
+    const double spc = fmax(w, 1e-12);
+    const double qq = (qa / spc) * n.ucf_flow;
+    int idx = 0;
+    while (idx < np && X[idx] < qq) ++idx;
+    const int k2 = min(max(idx, 1), np - 1), k1 = k2 - 1;
+    double rc = (Yc[k2] - Yc[k1]) / (X[k2] - X[k1]);
+    double h0c = Yc[k1] - rc * X[k1];
+    h0c = h0c / n.ucf_head;
+    rc = rc * n.ucf_flow / n.ucf_head;
+    dw = 2.0 * w * (-h0c) + (-rc) * q;
+    return;
+  }
+  const double pn = n.pn[k], H0 = th.h0(k), R = th.r(k);
+  if (t == 0) {  // CONST_HP: hloss = r / q on the unclamped branch only
+    const double r = R * pow(w, 2.0 - pn);
+    const double hgr = qa > 0.0 ? -r / qa / qa : kINF;
+    if (hgr > kCBIG || hgr < n.rqtol) return;
+    dw = (2.0 - pn) * R * pow(w, 1.0 - pn) / q;
+    dR = pow(w, 2.0 - pn) / q;
+    return;
+  }
+  dh0 = w * w;
+  if (pn == 1.0) {  // linear curve
+    dw = 2.0 * w * H0 + R * q;
+    dR = w * q;
+    return;
+  }
+  const double nm1 = pn - 1.0;
+  const double pw = qa == 0.0 ? (nm1 > 0.0 ? 0.0 : (nm1 < 0.0 ? kINF : 1.0)) : pow(qa, nm1);
+  const double hgr = pn * (R * pow(w, 2.0 - pn)) * pw;
+  if (hgr < n.rqtol) {  // RQtol clamp: hloss = h0 + RQtol q
+    dw = 2.0 * w * H0;
+    return;
+  }
+  dw = 2.0 * w * H0 + (2.0 - pn) * R * pow(w, 1.0 - pn) * pw * q;
+  dR = pow(w, 2.0 - pn) * pw * q;
 }
 
 // ---------------------------------------------------------------- linear algebra
@@ -861,12 +942,12 @@ __device__ void assemble_reduced(const DevNet& n, const TB& T, const Sh& s) {
 // Coefficients at the current state for polish / terminal (autodiff.py:786-875):
 // P, Y per link; emh per junction.
 template <int NT>
-__device__ void adj_coeffs(const DevNet& n, const Sh& s, const double* rrow,
+__device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const double* rrow,
                            const double* kerow) {
   const int tid = gtid<NT>();
   for (int k = tid; k < n.L; k += NT) {
     double P, Y;
-    link_coef(n, k, s.q[k], s.S[k], rrow[k], true, P, Y);
+    link_coef(n, th, k, s.q[k], s.S[k], rrow[k], true, P, Y);
     s.P[k] = P;
     s.Y[k] = Y;
   }
@@ -1112,6 +1193,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
   const double* kerow = a.ke + (long long)b * a.ke_stride;
   const double* drow = a.d + (long long)b * n.N;
   const double* rhrow = a.rh + (long long)b * n.N;
+  const PumpTh th = pump_th(n, a, b);
   for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     s.q[k] = a.q0 ? a.q0[(size_t)b * n.L + k] : n.q_init[k];
@@ -1135,7 +1217,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
     // ---- headloss coefficients
     for (int k = gtid<NT>(); k < n.L; k += NT) {
       double P, Y;
-      link_coef(n, k, s.q[k], s.S[k], rrow[k], false, P, Y);
+      link_coef(n, th, k, s.q[k], s.S[k], rrow[k], false, P, Y);
       s.P[k] = P;
       s.Y[k] = Y;
     }
@@ -1221,8 +1303,15 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
           else if (rev)
             st = WDS_CLOSED;
         }
-        if ((n.flags[k] & WDS_F_PUMP_LIVE) && st >= WDS_OPEN)  // pumpstatus
+        if (th.own_sp()) {  // pumpstatus at the call's speed (dgga/solver.py:673-679)
+          const double w = th.sp(k);
+          if (n.kind[k] == WDS_KIND_PUMP && w > 0.0 && st >= WDS_OPEN) {
+            const double hmax = (n.flags[k] & WDS_F_CHP) ? kBIG : w * w * n.phunit[k];
+            st = (-dh > hmax + n.htol) ? WDS_XHEAD : WDS_OPEN;
+          }
+        } else if ((n.flags[k] & WDS_F_PUMP_LIVE) && st >= WDS_OPEN) {  // pumpstatus
           st = (-dh > n.phmax[k] + n.htol) ? WDS_XHEAD : WDS_OPEN;
+        }
         const int t = n.link_tl[k];
         if (t >= 0) {  // tankstatus
           const bool live = st > WDS_CLOSED;
@@ -1267,7 +1356,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
     // small buffer: C [4p^2], y [2p], actf [p], row1 [p], then r_prv [p]
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
     for (int step = 0; step <= a.polish; ++step) {
-      adj_coeffs<NT>(n, s, rrow, kerow);
+      adj_coeffs<NT>(n, th, s, rrow, kerow);
       assemble_reduced<NT, FT>(n, T, s);
       if (!factor<NT, FT>(n, T, s)) {
         info = WDS_INFO_NOT_PD;
@@ -1345,13 +1434,18 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
         w.P[(size_t)b * n.L + k] = s.P[k];
         double dr = 0.0;
         const int st = s.S[k];
-        const bool closed = st <= WDS_CLOSED || (n.flags[k] & WDS_F_ZERO_SPEED);
+        const bool closed = st <= WDS_CLOSED || zero_speed(n, th, k, n.kind[k]);
         if ((n.flags[k] & WDS_F_IS_PIPE) && !closed) {
           const double sgn = q < 0.0 ? -1.0 : 1.0, qa = q * sgn;
           const double hgr = n.hexp * rrow[k] * pow(fmax(qa, 1e-30), n.hexp - 1.0);
           if (hgr >= n.rqtol) dr = pow(qa, n.hexp) * sgn;
         }
         w.dr[(size_t)b * n.L + k] = dr;
+        const int ip = n.link_pump[k];
+        if (ip >= 0) {
+          double* dp = w.dpump + (size_t)b * 3 * n.npump;
+          pump_dtheta(n, th, k, q, st, dp[ip], dp[n.npump + ip], dp[2 * n.npump + ip]);
+        }
       }
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
         const int es = s.eslot[p];
@@ -1565,6 +1659,19 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
     const double l1 = junc_of(T.e1[k], lam), l2 = junc_of(T.e2[k], lam);
     const double lam_l = s.P[k] * (gQ[k] - (l2 - l1));
     gr[k] = -(lam_l * dr[k]);
+    if (a.gsp) {  // pump theta (dgga/autodiff.py:736-741): -lam_l d hloss / d theta
+      const int ip = n.link_pump[k];
+      double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+      if (ip >= 0) {
+        const double* dp = w.dpump + (size_t)bf * 3 * n.npump;
+        g0 = -(lam_l * dp[ip]);
+        g1 = -(lam_l * dp[n.npump + ip]);
+        g2 = -(lam_l * dp[2 * n.npump + ip]);
+      }
+      a.gsp[(size_t)b * n.L + k] = g0;
+      a.gh0[(size_t)b * n.L + k] = g1;
+      a.grp[(size_t)b * n.L + k] = g2;
+    }
   }
   for (int f = gtid<NT>(); f < n.Nf; f += NT) {
     const int nd = n.fnode[f];

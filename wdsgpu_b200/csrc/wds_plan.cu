@@ -415,6 +415,19 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       q_init(net->q_init, net->q_init + L), ph0(net->pump_h0, net->pump_h0 + L),
       pr(net->pump_r, net->pump_r + L), pn(net->pump_n, net->pump_n + L),
       psp(net->pump_speed, net->pump_speed + L), phm(net->pump_hmax, net->pump_hmax + L);
+  // pump index of each link, and the pumpstatus shut-off head at unit speed
+  // (used when a call passes its own speeds)
+  std::vector<int> link_pump(L, -1);
+  std::vector<double> phu(L, 0.0);
+  int npump = 0;
+  for (int k = 0; k < L; ++k) {
+    if (kind[k] != WDS_KIND_PUMP) continue;
+    link_pump[k] = npump++;
+    if (net->pump_hunit)
+      phu[k] = net->pump_hunit[k];
+    else
+      phu[k] = psp[k] != 0.0 ? phm[k] / (psp[k] * psp[k]) : 0.0;
+  }
   std::vector<int> cptr(net->curve_ptr, net->curve_ptr + L + 1);
   std::vector<double> cx(net->curve_x, net->curve_x + cptr[L]), cy(net->curve_y, net->curve_y + cptr[L]);
   std::vector<double> el(Nj);
@@ -592,7 +605,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
          o_poff = blob.add(pcv_off), o_pxf = blob.add(pcv_xf), o_phs = blob.add(pcv_hset),
          o_pkm = blob.add(pcv_km), o_tll = blob.add(tl_link), o_tlt = blob.add(tl_tank),
          o_tlo = blob.add(tl_other), o_tlq = blob.add(tl_qsign), o_tlx = blob.add(tl_hmax),
-         o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags), o_stab = blob.add(stab_bytes);
+         o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags), o_stab = blob.add(stab_bytes),
+         o_lpu = blob.add(link_pump), o_phu = blob.add(phu);
   WdsPlan* plan = new WdsPlan();
   if (cudaMalloc(&plan->dtab, blob.bytes.size()) != cudaSuccess) {
     delete plan;
@@ -615,6 +629,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.km = P_(double, o_km); d.km_tcv = P_(double, o_kmt); d.q_init = P_(double, o_q0);
   d.ph0 = P_(double, o_ph0); d.pr = P_(double, o_pr); d.pn = P_(double, o_pn);
   d.pspeed = P_(double, o_psp); d.phmax = P_(double, o_phm); d.cptr = P_(int, o_cptr);
+  d.phunit = P_(double, o_phu); d.link_pump = P_(int, o_lpu); d.npump = npump;
   d.cx = P_(double, o_cx); d.cy = P_(double, o_cy); d.link_tl = P_(int, o_ltl);
   d.link_pcv = P_(int, o_lpcv); d.jnode = P_(int, o_jn); d.el = P_(double, o_el);
   d.inc_ptr = P_(int, o_incp); d.inc_split = P_(int, o_incs); d.inc = P_(int, o_inc);
@@ -684,7 +699,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
          oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
          oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4),
          olk = take(B * 2 * L * 8), otop = take(B * std::max(nT * nT, 1) * 8),
-         ostate = take(d.wide ? B * state_bytes : 0);
+         ostate = take(d.wide ? B * state_bytes : 0), opump = take(B * 3 * npump * 8);
   if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
     cudaFree(plan->dtab);
     delete plan;
@@ -697,6 +712,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
   w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
   w.state = d.wide ? wb + ostate : nullptr;
+  w.dpump = (double*)(wb + opump);
   // ---- host copy of the symbolic structure
   HostSym& hs = plan->sym;
   hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
@@ -725,6 +741,20 @@ extern "C" int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* co
   return WDS_OK;
 }
 
+namespace wds {
+// Pump parameters of a forward call: rows of [L] at stride 0 (one row for all
+// scenarios) or L (one per scenario).
+static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::string& who) {
+  a.th_sp = o->pump_speed;
+  a.th_h0 = o->pump_h0;
+  a.th_r = o->pump_r;
+  a.th_stride = o->pump_stride;
+  if ((o->pump_speed || o->pump_h0 || o->pump_r) && o->pump_stride != 0 && o->pump_stride != L)
+    return fail(WDS_E_ARG, who + ": pump_stride must be 0 or n_links");
+  return WDS_OK;
+}
+}  // namespace wds
+
 extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o,
                            const double* demand, const double* fixed_head, const double* ke,
                            const double* r, double* head, double* flow, double* emitter,
@@ -743,6 +773,7 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
   a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
   a.q0 = o->q0; a.e0 = o->e0;
+  if (int rc0 = set_pump_opts(a, o, plan->dn.L, "wds_forward"); rc0 != WDS_OK) return rc0;
   a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
   a.relerr = relerr; a.info = info;
   std::string err;
@@ -808,6 +839,9 @@ extern "C" int wds_forward_multi(int32_t nplans, WdsPlan* const* plans, const in
     a.sm = o->status_machine ? 1 : 0; a.refine = o->refine; a.polish = o->polish_steps;
     a.ke_stride = o->ke_stride; a.r_stride = o->r_stride;
     a.d = x.demand; a.rh = x.fixed_head; a.ke = x.ke; a.r = x.r; a.q0 = o->q0; a.e0 = o->e0;
+    if (int rc0 = set_pump_opts(a, o, plan->dn.L, "wds_forward_multi: plan " + std::to_string(p));
+        rc0 != WDS_OK)
+      return rc0;
     a.head = x.head; a.flow = x.flow; a.emit = x.emitter; a.status = x.status;
     a.iters = x.iters; a.relerr = x.relerr; a.info = x.info;
   }
@@ -857,6 +891,27 @@ extern "C" int wds_adjoint(WdsPlan* plan, int32_t batch, const double* gH, const
   if (!plan->have_state || batch != plan->state_batch)
     return fail(WDS_E_STATE, "wds_adjoint: no implicit forward of this batch size to differentiate");
   AdjArgs a{batch, gH, gQ, gE, gd, grh, gke, gr};
+  std::string err;
+  int rc = launch_adjoint(plan->dn, plan->dw, a, plan->groups, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  return WDS_OK;
+}
+
+extern "C" int wds_adjoint_pumps(WdsPlan* plan, int32_t batch, const double* gH,
+                                 const double* gQ, const double* gE, double* gd, double* grh,
+                                 double* gke, double* gr, double* gspeed, double* gh0,
+                                 double* grp, void* stream) {
+  using namespace wds;
+  if (!plan || batch <= 0 || !gH || !gQ || !gE || !gd || !grh || !gke || !gr || !gspeed ||
+      !gh0 || !grp)
+    return fail(WDS_E_ARG, "wds_adjoint_pumps: bad argument");
+  if (!plan->have_state || batch != plan->state_batch)
+    return fail(WDS_E_STATE,
+                "wds_adjoint_pumps: no implicit forward of this batch size to differentiate");
+  AdjArgs a{batch, gH, gQ, gE, gd, grh, gke, gr};
+  a.gsp = gspeed;
+  a.gh0 = gh0;
+  a.grp = grp;
   std::string err;
   int rc = launch_adjoint(plan->dn, plan->dw, a, plan->groups, stream, &err);
   if (rc != WDS_OK) return fail(rc, err);
@@ -940,7 +995,8 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
                oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
                oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4),
                olk = take(B * 2 * d.L * 8), otop = take(B * std::max(d.nT * d.nT, 1) * 8),
-               ostate = take(d.wide ? B * state_smem_bytes(d) : 0);
+               ostate = take(d.wide ? B * state_smem_bytes(d) : 0),
+               opump = take(B * 3 * d.npump * 8);
   if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
     const size_t per = bytes / B;
     return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
@@ -959,12 +1015,15 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
   w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
   w.state = d.wide ? wb + ostate : nullptr;
+  w.dpump = (double*)(wb + opump);
   w.nscr = nscr;
   FwdArgs a{};
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
   a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;
   a.r_stride = o->r_stride; a.d = demand; a.rh = fixed_head; a.ke = ke; a.r = r;
   a.q0 = o->q0; a.e0 = o->e0;
+  rc = set_pump_opts(a, o, d.L, "wds_forward_noalloc");
+  if (rc != WDS_OK) return rc;
   a.head = head; a.flow = flow; a.emit = emitter; a.status = status; a.iters = iters;
   a.relerr = relerr; a.info = info;
   std::string err;

@@ -41,14 +41,16 @@ def sensitivity_matrix(solver, demand, res_head, r_hw, sensor_nodes, wrt="C", fr
                        ke=None, accuracy=1e-12, max_iter=200, polish_steps=3, speed=None,
                        status=None, pump_h0=None, pump_r=None, return_info=False):
     """S[T*m, L] = dp_sensor/dtheta, theta = C (roughness) or r (r_hw), rows
-    frame-major ([frame 0's m rows; frame 1's m rows; ...]), as the reference."""
+    frame-major ([frame 0's m rows; frame 1's m rows; ...]), as the reference.
+    speed / pump_h0 / pump_r ([L] or [T, L]) set the frames' pump parameters
+    as in implicit_solve."""
     s = solver
     if wrt not in ("C", "r"):
         raise ValueError("wrt must be 'C' or 'r'")
-    if speed is not None or status is not None or pump_h0 is not None or pump_r is not None:
+    if status is not None:
         raise NotImplementedError(
-            "speed/status/pump_h0/pump_r are not taken by the B200 route (the status "
-            "machine decides the status; pump parameters stay the network's)")
+            "status is not taken by the B200 route (the batched status machine decides "
+            "each frame's status)")
     sensors = np.asarray(sensor_nodes, dtype=np.int64).ravel()
     nt = np.asarray(s.net.node_type)
     bad = sensors[nt[sensors] != 0]
@@ -60,8 +62,9 @@ def sensitivity_matrix(solver, demand, res_head, r_hw, sensor_nodes, wrt="C", fr
     ke = s.node_ke_default if ke is None else ke
     r_hw = s.r_hw if r_hw is None else r_hw
     d, rh, ke_t, r_t, B, _ = s._inputs(demand, res_head, ke, r_hw)
+    pumps = s.pump_rows(B, speed, pump_h0, pump_r)
     o = s.run(d, rh, ke_t.contiguous(), r_t.contiguous(), B, int(max_iter), float(accuracy),
-              True, int(polish_steps))
+              True, int(polish_steps), pumps=pumps)
     info_v = o["info"]
     _check_emitter_cap(s, info_v)
     if bool((info_v != 0).any()):

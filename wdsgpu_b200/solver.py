@@ -56,7 +56,7 @@ class _Plan:
         net.link_kind = _ptr(t["kind"], ctypes.c_int8)
         net.link_flags = _ptr(t["flags"], ctypes.c_uint8)
         for f in ("km", "km_tcv", "q_init", "pump_h0", "pump_r", "pump_n",
-                  "pump_speed", "pump_hmax", "curve_x", "curve_y", "prv_hset",
+                  "pump_speed", "pump_hmax", "pump_hunit", "curve_x", "curve_y", "prv_hset",
                   "tl_qsign", "tl_hmax", "tl_hmin"):
             setattr(net, f, _ptr(t[f], ctypes.c_double))
         net.status0 = _ptr(t["status0"], ctypes.c_int8)
@@ -376,7 +376,8 @@ class GGASolver:
             n1=c32(n1), n2=c32(n2), kind=kind, flags=flags, km=c64(km),
             km_tcv=c64(km_tcv), q_init=c64(q_init), status0=status0,
             pump_type=ptype, pump_h0=c64(ph0), pump_r=c64(pr), pump_n=c64(pn),
-            pump_speed=c64(sp), pump_hmax=c64(pump_hmax), curve_ptr=curve_ptr,
+            pump_speed=c64(sp), pump_hmax=c64(pump_hmax),
+            pump_hunit=c64(np.where(chp, BIG, phm)), curve_ptr=curve_ptr,
             curve_x=c64(cx if cx else [0.0]), curve_y=c64(cy if cy else [0.0]),
             prv_hset=c64(prv_hset), tl_link=c32(kk), tl_tank=c32(tank),
             tl_other=c32(np.where(use_n2[kk], n1[kk], n2[kk])),
@@ -495,11 +496,49 @@ class GGASolver:
         if record_schedule:
             raise NotImplementedError("record_schedule is not provided by the sm100 route")
 
+    def pump_rows(self, B, speed=None, pump_h0=None, pump_r=None):
+        """Pump parameters of a call as FP64 device rows: (speed, h0, r), each
+        None or [1, L] / [B, L] with one common row count (an [L] row next to
+        [B, L] rows is expanded).  Values off pump links are not read."""
+        vals = [speed, pump_h0, pump_r]
+        if all(v is None for v in vals):
+            return None
+        dev, L = self.device, self.L
+        out = []
+        for name, v in zip(("speed", "pump_h0", "pump_r"), vals):
+            if v is None:
+                out.append(None)
+                continue
+            t = v.detach() if isinstance(v, torch.Tensor) else torch.as_tensor(np.asarray(v))
+            t = t.to(dtype=torch.float64, device=dev)
+            if t.dim() == 1:
+                t = t.unsqueeze(0)
+            if t.dim() != 2 or t.shape[1] != L or t.shape[0] not in (1, B):
+                raise ValueError("%s must be [L] or [B, L] (L=%d, B=%d), got %s"
+                                 % (name, L, B, tuple(t.shape)))
+            if name == "speed":
+                # the reference's speed is the whole link-setting vector
+                # (LinkSetting, dgga/autodiff.py:99-120); off pump links it
+                # would set valve settings, which this route does not take
+                off = self._lt != PUMP
+                host = t.cpu().numpy()
+                bad = np.flatnonzero((host[:, off] != self.init_setting[off]).any(0))
+                if bad.size:
+                    raise NotImplementedError(
+                        "speed differs from the network's link settings off pump links "
+                        "(links %s): valve settings are not parameters of this route"
+                        % np.flatnonzero(off)[bad][:8].tolist())
+            out.append(t)
+        rows = max(t.shape[0] for t in out if t is not None)
+        return tuple(None if t is None else t.expand(rows, L).contiguous() for t in out)
+
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
-            refine=None, plan=None, q0=None, e0=None):
+            refine=None, plan=None, q0=None, e0=None, pumps=None):
         """One wds_forward call on device tensors; returns the raw outputs.
         q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
-        warm start of GGASolver.solve (dgga/solver.py:2876-2887)."""
+        warm start of GGASolver.solve (dgga/solver.py:2876-2887); pumps is
+        the (speed, h0, r) of `pump_rows` (the call's pump parameters, or
+        None for the network's)."""
         p = plan or self.plan(B)
         dev = self.device
         head = torch.empty(B, self.N, dtype=torch.float64, device=dev)
@@ -526,6 +565,12 @@ class GGASolver:
                     raise ValueError("%s must be a contiguous float64 [%d, %d] tensor on %s"
                                      % (name, B, cols, dev))
                 setattr(o, name, t.data_ptr())
+        if pumps is not None:
+            rows = next(t.shape[0] for t in pumps if t is not None)
+            o.pump_stride = 0 if rows == 1 else self.L
+            for name, t in zip(("pump_speed", "pump_h0", "pump_r"), pumps):
+                if t is not None:
+                    setattr(o, name, t.data_ptr())
         cur = torch.cuda.current_stream(dev)
         stream = cur.cuda_stream
         ev = self._event_pair(cur, "forward")
@@ -537,7 +582,7 @@ class GGASolver:
         if ev is not None:
             ev[1].record(cur)
         return dict(head=head, flow=flow, emit=emit, status=status, iters=iters,
-                    relerr=relerr, info=info, plan=p)
+                    relerr=relerr, info=info, plan=p, pumps=pumps)
 
     def solve(self, demand_cfs, res_head_ft, ke_int=None, q0=None, e0=None,
               max_iter=None, accuracy=None, link_status=None, link_setting=None,
