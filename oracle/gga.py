@@ -352,6 +352,26 @@ class Model:
                 dR[b, k] = w ** (2.0 - n) * pw * qk
         return dw, dh0, dR
 
+    def chp_clamp(self, q, S):
+        """[B,L] mask of open constant-HP pumps on their CBIG / RQtol clamp
+        branch (hydcoeffs.c:748-757): there hloss = -hgrad q, so the exact
+        d hloss / dq of the CPU adjoint is -hgrad (autodiff.py:186-193) where
+        the GGA matrix assembles +hgrad."""
+        B = q.shape[0]
+        out = np.zeros((B, self.L), dtype=bool)
+        for k in np.flatnonzero(self.is_pump & self.p_chp):
+            w = float(self.speed[k])
+            if w == 0.0:
+                continue
+            re = self.p_r[k] * max(w, 1e-12) ** (2.0 - self.p_n[k])
+            for b in range(B):
+                if S is not None and S[b, k] <= CLOSED:
+                    continue
+                qa = max(abs(float(q[b, k])), 1e-30)
+                raw = -re / qa / qa
+                out[b, k] = raw > CBIG or raw < self.rqtol
+        return out
+
     def emitter(self, e, ke):
         """Emitter head loss and gradient (solver.py:2368-2377)."""
         kea = np.maximum(ke, CSMALL)
@@ -651,9 +671,10 @@ class Model:
                 np.add.at(out[b], self.prv_j2, x[b, self.prv_j2] * act[b] * CBIG)
         return out
 
-    def factor(self, P, emh, act):
+    def factor(self, P, emh, act, lu=False):
         """Assemble the reduced matrix at the current state and factor it
-        (autodiff.py:928-962)."""
+        (autodiff.py:928-962); lu: an LU factor, for the indefinite matrix of
+        the exact Jacobian with clamped constant-HP pumps."""
         B, Nj = P.shape[0], self.Nj
         vals = np.concatenate([-P[:, self.lk_both], -P[:, self.lk_both],
                                P[:, self.lk_m1], P[:, self.lk_m2]], axis=1)
@@ -664,11 +685,14 @@ class Model:
             for b in range(B):
                 np.add.at(A[b], self.prv_j2 * (Nj + 1), CBIG * act[b])
         A = A.reshape(B, Nj, Nj)
+        if lu:
+            return [("lu", sla.lu_factor(A[b])) for b in range(B)]
         return [sla.cho_factor(A[b], lower=True) for b in range(B)]
 
     @staticmethod
     def _fsolve(kf, rhs):
-        return np.stack([sla.cho_solve(kf[b], rhs[b]) for b in range(rhs.shape[0])])
+        return np.stack([sla.lu_solve(kf[b][1], rhs[b]) if isinstance(kf[b][0], str)
+                         else sla.cho_solve(kf[b], rhs[b]) for b in range(rhs.shape[0])])
 
     def _solveA(self, kf, P, emh, act, rhs, n_ref=2):
         x = self._fsolve(kf, rhs)
@@ -796,6 +820,10 @@ class Model:
         pumps: also the pump-theta gradients (d speed, d H0, d R) [B,L]."""
         B = q.shape[0]
         P, _, emh, hge, em, dr, dke, act = self.adj_coeffs(q, e, ke, r, S)
+        clamp = self.chp_clamp(q, S)
+        if clamp.any():   # exact Jacobian: -hgrad on the clamp branch
+            P = np.where(clamp, -P, P)
+            kf = self.factor(P, emh, act, lu=True)
         gHj, gEj = gH[:, self.junc], gE[:, self.junc]
         PgQ = P * gQ
         rr = _scatter(self.Nj, self.f2, PgQ[:, self.lk_m2])

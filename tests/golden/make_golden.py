@@ -18,7 +18,8 @@ and the reference outputs of
 Usage:  python tests/golden/make_golden.py        (steady cases)
         python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
         python tests/golden/make_golden.py sens   (sensitivity-matrix pin, sens_ref.npz)
-        python tests/golden/make_golden.py pumps  (pump-parameter gradient pin, pump_ref.npz)
+        python tests/golden/make_golden.py pumps  (pump-parameter gradient pins, pump_ref.npz
+                                                   and chp_ref.npz)
 """
 import json
 import os
@@ -263,15 +264,67 @@ def make_sens():
                                                   os.path.basename(path)))
 
 
+def _pump_case(dgga, torch, net, d, rh, speed_scale, h0_scale, r_scale, name):
+    """The reference's CPU implicit adjoint with pump theta (ImplicitGGASolve,
+    dgga/autodiff.py:609-756: speed / pump_h0 / pump_r as differentiable [L]
+    tensors, statuses frozen), one scenario per call (the statuses are per
+    scenario), each scenario given the statuses of the reference's own dense
+    status machine.  The loss is the sum of squared heads at the sensors and
+    at the pumps' downstream nodes plus the sum of squared pump flows."""
+    ke = np.asarray(net.node_ke, dtype=np.float64)
+    sens = synth_sensor_nodes(net)
+    ref_net = dgga.parse.Net(**net.as_fields())
+    se = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
+    pl = np.asarray(net.pump_link, dtype=np.int64)
+    pn2 = np.asarray(net.link_n2, dtype=np.int64)[pl]
+    speed = np.asarray(se.init_setting, dtype=np.float64).copy()
+    speed[pl] = speed[pl] * np.asarray(speed_scale)
+    h0 = np.asarray(se.pl_h0, dtype=np.float64).copy()
+    h0[pl] = h0[pl] * np.asarray(h0_scale)
+    rp = np.asarray(se.pl_r, dtype=np.float64).copy()
+    rp[pl] = rp[pl] * np.asarray(r_scale)
+    dn = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
+    st = dn.solve(torch.tensor(d), torch.tensor(rh), status_machine=True, accuracy=1e-10,
+                  assemble="csr", linear_solver="dense")["status"].numpy()
+    keys = ("head", "flow", "g_speed", "g_h0", "g_r", "g_demand", "g_rhw", "g_res_head")
+    res = {k: [] for k in keys}
+    for b in range(d.shape[0]):
+        D = torch.tensor(d[b:b + 1]).requires_grad_(True)
+        RH = torch.tensor(rh[b:b + 1]).requires_grad_(True)
+        R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+        sp = torch.tensor(speed).requires_grad_(True)
+        h0t = torch.tensor(h0).requires_grad_(True)
+        rpt = torch.tensor(rp).requires_grad_(True)
+        h, q, e = dgga.autodiff.implicit_solve(
+            se, D, RH, ke=torch.tensor(ke), r_hw=R, accuracy=1e-10,
+            adjoint="cpu", speed=sp, pump_h0=h0t, pump_r=rpt, status=st[b])
+        loss = (h[:, sens] ** 2).sum() + (h[:, pn2] ** 2).sum() + (q[:, pl] ** 2).sum()
+        loss.backward()
+        for k, v in zip(keys, (h.detach(), q.detach(), sp.grad, h0t.grad, rpt.grad, D.grad,
+                               R.grad, RH.grad)):
+            res[k].append(np.asarray(v).reshape(-1))
+    blob = pack_net(net)
+    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
+                 "in_speed": speed, "in_pump_h0": h0, "in_pump_r": rp, "in_status": st})
+    blob.update({"ref_" + k: np.stack(v) for k, v in res.items()})
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **blob)
+    print("%s: g_speed at pumps %s -> %s" % (
+        name, np.stack(res["g_speed"])[:, pl].tolist(), os.path.basename(path)))
+
+
+def synth_sensor_nodes(net):
+    from wdsgpu_b200 import synth
+    return synth.sensor_nodes(net, 6)
+
+
 def make_pumps():
-    """Pump-parameter pin: the reference's CPU implicit adjoint with pump theta
-    (ImplicitGGASolve, dgga/autodiff.py:609-756: speed / pump_h0 / pump_r as
-    differentiable [L] tensors, statuses frozen) on the feature network with
-    all four pump kinds (power function, custom curve, no curve, constant HP),
-    at speeds and curve coefficients moved off the network's values.  One
-    scenario per call (the statuses are per scenario); the loss is the sum of
-    squared heads at the sensors and at the pumps' downstream nodes plus the
-    sum of squared pump flows."""
+    """Pump-parameter pins.  pump_ref: the feature network with all four pump
+    kinds (power function, custom curve, no curve, constant HP) at speeds and
+    curve coefficients moved off the network's values.  chp_ref: the same
+    network with its constant-HP pump feeding a dead end of tiny demand, so
+    that the pump sits on its CBIG clamp branch (hydcoeffs.c:748-752) at the
+    converged state."""
     import torch
     sys.path.insert(0, REPO)
     from wdsgpu_b200 import synth
@@ -280,46 +333,13 @@ def make_pumps():
     net = synth.feature_network(tank_level=0.5, with_chp=True)
     d, _ = synth.config2_scenarios(net, 3, seed=17, sigma=0.3)
     rh = np.broadcast_to(net.fixed_head_ft_at(0), d.shape).copy()
-    ke = np.asarray(net.node_ke, dtype=np.float64)
-    sens = synth.sensor_nodes(net, 6)
-    ref_net = dgga.parse.Net(**net.as_fields())
-    se = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
-    pl = np.asarray(net.pump_link, dtype=np.int64)
-    pn2 = np.asarray(net.link_n2, dtype=np.int64)[pl]
-    speed = np.asarray(se.init_setting, dtype=np.float64).copy()
-    speed[pl] = speed[pl] * np.array([0.97, 1.04, 1.0, 1.02])
-    h0 = np.asarray(se.pl_h0, dtype=np.float64).copy()
-    h0[pl[0]] *= 1.03
-    rp = np.asarray(se.pl_r, dtype=np.float64).copy()
-    rp[pl[0]] *= 0.95
-    rp[pl[3]] *= 1.05
-    dn = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
-    st = dn.solve(torch.tensor(d), torch.tensor(rh), status_machine=True, accuracy=1e-10,
-                  assemble="csr", linear_solver="dense")["status"].numpy()
-    keys = ("head", "flow", "g_speed", "g_h0", "g_r", "g_demand", "g_rhw")
-    res = {k: [] for k in keys}
-    for b in range(d.shape[0]):
-        D = torch.tensor(d[b:b + 1]).requires_grad_(True)
-        R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
-        sp = torch.tensor(speed).requires_grad_(True)
-        h0t = torch.tensor(h0).requires_grad_(True)
-        rpt = torch.tensor(rp).requires_grad_(True)
-        h, q, e = dgga.autodiff.implicit_solve(
-            se, D, torch.tensor(rh[b:b + 1]), ke=torch.tensor(ke), r_hw=R, accuracy=1e-10,
-            adjoint="cpu", speed=sp, pump_h0=h0t, pump_r=rpt, status=st[b])
-        loss = (h[:, sens] ** 2).sum() + (h[:, pn2] ** 2).sum() + (q[:, pl] ** 2).sum()
-        loss.backward()
-        for k, v in zip(keys, (h.detach(), q.detach(), sp.grad, h0t.grad, rpt.grad, D.grad,
-                               R.grad)):
-            res[k].append(np.asarray(v).reshape(-1))
-    blob = pack_net(net)
-    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
-                 "in_speed": speed, "in_pump_h0": h0, "in_pump_r": rp, "in_status": st})
-    blob.update({"ref_" + k: np.stack(v) for k, v in res.items()})
-    path = os.path.join(HERE, "pump_ref.npz")
-    np.savez_compressed(path, **blob)
-    print("pumps: g_speed at pumps %s -> %s" % (
-        np.stack(res["g_speed"])[:, pl].tolist(), os.path.basename(path)))
+    _pump_case(dgga, torch, net, d, rh, [0.97, 1.04, 1.0, 1.02], [1.03, 1, 1, 1],
+               [0.95, 1, 1, 1.05], "pump_ref")
+    net = synth.chp_dead_end_network()
+    d, _ = synth.config2_scenarios(net, 3, seed=17, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    _pump_case(dgga, torch, net, d, rh, [0.97, 1.0, 1.0, 1.02], [1, 1, 1, 1],
+               [1, 1, 1, 1.05], "chp_ref")
 
 
 if __name__ == "__main__":

@@ -34,35 +34,48 @@ def _gpu_loss_grads(s, net, inp, th, cuda, per_row=False):
             t = t.unsqueeze(0).expand(B, -1).contiguous()
         ts.append(t.requires_grad_(True))
     D = torch.tensor(inp["demand"], device=cuda).requires_grad_(True)
-    h, q, e = implicit_solve(s, D, torch.tensor(inp["res_head"], device=cuda),
-                             ke=torch.tensor(inp["ke"], device=cuda), accuracy=1e-7,
+    RH = torch.tensor(np.nan_to_num(inp["res_head"]), device=cuda).requires_grad_(True)
+    h, q, e = implicit_solve(s, D, RH, ke=torch.tensor(inp["ke"], device=cuda), accuracy=1e-7,
                              speed=ts[0], pump_h0=ts[1], pump_r=ts[2])
     sens = torch.as_tensor(np.asarray(inp["sensors"]), device=cuda)
     loss = (h[:, sens] ** 2).sum() + (h[:, torch.as_tensor(pn2, device=cuda)] ** 2).sum() \
         + (q[:, torch.as_tensor(pl, device=cuda)] ** 2).sum()
     loss.backward()
+    _gpu_loss_grads.g_res_head = RH.grad.cpu().numpy()
     return h.detach().cpu().numpy(), q.detach().cpu().numpy(), D.grad.cpu().numpy(), \
         [t.grad.cpu().numpy() for t in ts]
 
 
-def test_pump_theta_matches_reference(cuda):
+@pytest.mark.parametrize("case", ["pump_ref", "chp_ref"])
+def test_pump_theta_matches_reference(cuda, case):
+    """pump_ref: all four pump kinds at moved parameters; chp_ref: a
+    constant-HP pump on its CBIG clamp branch (exact Jacobian by the Woodbury
+    correction on the kept factor).  In chp_ref the dead-end junction hangs on
+    the pump's 1/CBIG conductance, so the reduced system has a condition
+    number near 1e10 and the gradient at that junction (4e12) agrees to about
+    1e-8 relative; elsewhere to 1e-10."""
     from wdsgpu_b200.solver import GGASolver
-    net, inp, ref = load("pump_ref")
+    net, inp, ref = load(case)
+    tol = 1e-8 if case == "pump_ref" else 1e-7
     s = GGASolver(net, device=cuda, dense_status_machine=True)
     th = (inp["speed"], inp["pump_h0"], inp["pump_r"])
     # [L] rows shared by the batch: the batch-summed gradient, as the reference
     h, q, gd, g = _gpu_loss_grads(s, net, inp, th, cuda)
-    assert np.abs(h - ref["head"]).max() < 1e-9
-    assert np.abs(gd - ref["g_demand"]).max() <= 1e-8 * np.abs(ref["g_demand"]).max()
+    assert np.abs(h - ref["head"]).max() <= 1e-9 * max(np.abs(ref["head"]).max(), 1e3)
+    assert np.abs(gd - ref["g_demand"]).max() <= tol * np.abs(ref["g_demand"]).max()
+    grh = _gpu_loss_grads.g_res_head
+    fixed = np.asarray(net.node_type) != 0
+    R = ref["g_res_head"][:, fixed]
+    assert np.abs(grh[:, fixed] - R).max() <= tol * np.abs(R).max()
     for gi, key in zip(g, ("g_speed", "g_h0", "g_r")):
         R = ref[key].sum(0)
-        assert np.abs(gi - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi - R).max())
+        assert np.abs(gi - R).max() <= tol * np.abs(R).max(), (key, np.abs(gi - R).max())
     # [B,L] rows: one gradient row per scenario
     _, _, _, g = _gpu_loss_grads(s, net, inp, th, cuda, per_row=True)
     for gi, key in zip(g, ("g_speed", "g_h0", "g_r")):
         R = ref[key]
         assert gi.shape == R.shape
-        assert np.abs(gi - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi - R).max())
+        assert np.abs(gi - R).max() <= tol * np.abs(R).max(), (key, np.abs(gi - R).max())
 
 
 def test_network_values_are_the_default(cuda):

@@ -43,8 +43,8 @@ def test_oracle_pump_theta_matches_reference():
     out, _, g = pump_loss_grads(m, net, inp)
     assert (out["status"] == inp["status"]).all()
     assert np.abs(out["head_ft"] - ref["head"]).max() < 1e-9
-    for gi, key in ((g[0], "g_demand"), (g[3], "g_rhw"), (g[4], "g_speed"), (g[5], "g_h0"),
-                    (g[6], "g_r")):
+    for gi, key in ((g[0], "g_demand"), (g[1], "g_res_head"), (g[3], "g_rhw"), (g[4], "g_speed"),
+                    (g[5], "g_h0"), (g[6], "g_r")):
         R = ref[key]
         assert np.abs(gi - R).max() <= 1e-9 * np.abs(R).max(), (key, np.abs(gi - R).max())
     pl = np.asarray(net.pump_link)
@@ -74,3 +74,24 @@ def test_oracle_pump_theta_finite_difference():
         fd = (vals[0] - vals[1]) / (2.0 * eps)
         an = g[4 + which][0, k]
         assert abs(fd - an) <= 1e-5 * max(abs(an), 1.0), (which, k, fd, an)
+
+
+def test_oracle_chp_clamp_matches_reference():
+    """A constant-HP pump feeding a dead end of tiny demand sits on its CBIG
+    clamp branch; the exact Jacobian there (-CBIG where the GGA matrix has
+    +CBIG, dgga/autodiff.py:186-193) gives the reference's CPU-adjoint
+    gradients (fixture tests/golden/chp_ref.npz), and the assembled one does
+    not."""
+    net, inp, ref = load("chp_ref")
+    m = Model(net).with_pumps(inp["speed"], inp["pump_h0"], inp["pump_r"])
+    out, _, g = pump_loss_grads(m, net, inp)
+    assert (out["status"] == inp["status"]).all()
+    pl = np.asarray(net.pump_link)
+    assert m.chp_clamp(out["flow_cfs"], out["status"])[:, pl[3]].all()
+    for gi, key in ((g[0], "g_demand"), (g[1], "g_res_head"), (g[3], "g_rhw"), (g[4], "g_speed"),
+                    (g[5], "g_h0"), (g[6], "g_r")):
+        R = ref[key]
+        assert np.abs(gi - R).max() <= 1e-9 * np.abs(R).max(), (key, np.abs(gi - R).max())
+    m.chp_clamp = lambda q, S: np.zeros(q.shape, dtype=bool)      # the assembled Jacobian
+    _, _, g = pump_loss_grads(m, net, inp)
+    assert np.abs(g[0] - ref["g_demand"]).max() > 0.5 * np.abs(ref["g_demand"]).max()

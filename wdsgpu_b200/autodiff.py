@@ -17,9 +17,13 @@ forward keeps d hloss / d theta of every pump at the terminal state and
 `wds_adjoint_pumps` contracts it with the link adjoint, the formulas of the
 reference's CPU adjoint (dgga/autodiff.py:122-218, 736-741).
 
+Constant-HP pumps on their CBIG / RQtol clamp branch, which the reference's
+GPU route refuses (its assembled +hgrad is not the exact -hgrad of the CPU
+adjoint, dgga/autodiff.py:186-193), are differentiated exactly: a Woodbury
+correction on the kept factor (`_clamp_rhs`), only when such a pump exists.
+
 Refusals follow the reference: unconverged scenarios, second derivatives,
-a frozen `status`, constant-HP pumps on their clamp branch, PRVs that share a
-downstream junction or cascade.
+a frozen `status`, PRVs that share a downstream junction or cascade.
 """
 from __future__ import annotations
 
@@ -34,9 +38,14 @@ from .solver import CBIG, GGASolver, _not_pd_hint
 __all__ = ["implicit_solve", "ImplicitGGASolveSM100", "hw_resistance", "dr_dC"]
 
 
-def _adjoint_guards(s: GGASolver, flow, S, pumps=None):
+def _adjoint_guards(s: GGASolver, flow, S, pumps=None, allow_clamp=False):
     """Refusals of the reduced adjoint (dgga/autodiff.py:1157-1170); pumps is
-    the call's (speed, h0, r) rows of GGASolver.pump_rows, or None."""
+    the call's (speed, h0, r) rows of GGASolver.pump_rows, or None.
+
+    Open constant-HP pumps on their CBIG / RQtol clamp branch
+    (hydcoeffs.c:748-757) are refused unless allow_clamp; then the clamped
+    entries are returned as (scenario, link, assembled P) tensors (None when
+    there are none) for `_clamp_rhs`."""
     if s.n_pcv:
         j1 = s._n1[s.pcv_links]
         j2 = s._n2[s.pcv_links]
@@ -48,27 +57,116 @@ def _adjoint_guards(s: GGASolver, flow, S, pumps=None):
                 "adjoint='gpu': cascaded PRVs (a downstream junction is another "
                 "PRV's upstream junction)")
     chp = s._tables["pump_type"] == 0
-    if chp.any():
-        t = s._tables
-        ks = np.flatnonzero(chp)
-        dev = flow.device
-        kt = torch.as_tensor(ks, device=dev)
-        q = flow.index_select(1, kt)
-        sgn = torch.where(q < 0, -1.0, 1.0)
-        qa = (q * sgn).clamp_min(1e-30)
-        sp_row = (pumps[0].index_select(1, kt) if pumps is not None and pumps[0] is not None
-                  else torch.as_tensor(t["pump_speed"][ks], device=dev))
-        r_row = (pumps[2].index_select(1, kt) if pumps is not None and pumps[2] is not None
-                 else torch.as_tensor(t["pump_r"][ks], device=dev))
-        sp = sp_row.clamp_min(1e-12)
-        re = r_row * sp ** (2.0 - torch.as_tensor(t["pump_n"][ks], device=dev))
-        raw = -re / qa / qa
-        closed = (S.index_select(1, kt) <= 2) | (sp_row == 0.0)
-        bad = ~closed & ((raw > CBIG) | (raw < s.rqtol))
-        if bool(bad.any()):
-            raise NotImplementedError(
-                "adjoint='gpu': a constant-HP pump sits on its CBIG/RQtol clamp "
-                "branch at the converged state")
+    if not chp.any():
+        return None
+    t = s._tables
+    ks = np.flatnonzero(chp)
+    dev = flow.device
+    kt = torch.as_tensor(ks, device=dev)
+    q = flow.index_select(1, kt)
+    sgn = torch.where(q < 0, -1.0, 1.0)
+    qa = (q * sgn).clamp_min(1e-30)
+    sp_row = (pumps[0].index_select(1, kt) if pumps is not None and pumps[0] is not None
+              else torch.as_tensor(t["pump_speed"][ks], device=dev))
+    r_row = (pumps[2].index_select(1, kt) if pumps is not None and pumps[2] is not None
+             else torch.as_tensor(t["pump_r"][ks], device=dev))
+    sp = sp_row.clamp_min(1e-12)
+    re = r_row * sp ** (2.0 - torch.as_tensor(t["pump_n"][ks], device=dev))
+    raw = -re / qa / qa
+    closed = (S.index_select(1, kt) <= 2) | (sp_row == 0.0)
+    big = ~closed & (raw > CBIG)
+    bad = big | (~closed & (raw < s.rqtol))
+    if not bool(bad.any()):
+        return None
+    if not allow_clamp:
+        raise NotImplementedError(
+            "adjoint='gpu': a constant-HP pump sits on its CBIG/RQtol clamp "
+            "branch at the converged state")
+    b_idx, j_idx = torch.nonzero(bad, as_tuple=True)
+    pf = torch.where(big[b_idx, j_idx], 1.0 / CBIG, 1.0 / s.rqtol).to(torch.float64)
+    return b_idx, kt[j_idx], pf
+
+
+def _clamp_rhs(s: GGASolver, plan, B, clamp, gH, gQ, gE, stream):
+    """Adjoint right-hand side for clamped constant-HP pumps.
+
+    On the clamp branch hloss = -hgrad q, so the exact Jacobian of the CPU
+    adjoint has -hgrad where the kept factor assembled +hgrad
+    (dgga/autodiff.py:186-193): the true reduced operator is the kept one
+    plus sum_c dP_c a_c a_c^T (a_c the link's junction incidence,
+    dP_c = -2 P_c).  By Woodbury, lambda_true = M^{-1}(r - U z) with
+    z = (diag(1/dP) + V^T X)^{-1} V^T lambda, X = M^{-1} a_c (one kept-factor
+    solve per clamped pump, `wds_adjoint_rhs`) and lambda = M^{-1} r (one
+    `wds_adjoint`).  Since r = B^T P gQ - em gE / hge - gH, the returned gH' =
+    gH + U z makes the next adjoint launch produce every gradient from
+    lambda_true.  Also returns (b, k, dP) for `_clamp_grh`."""
+    b_idx, k_idx, pf = clamp
+    dev = gH.device
+    N, L = s.N, s.L
+    dP = -2.0 * pf
+    # lambda of the kept operator: gd holds it at the junctions (0 at fixed nodes)
+    lam = torch.empty(B, N, dtype=torch.float64, device=dev)
+    t1, t2, t3 = torch.empty_like(lam), torch.empty_like(lam), torch.empty(B, L, dtype=torch.float64,
+                                                                           device=dev)
+    _lib.check(plan.lib.wds_adjoint(
+        plan.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), lam.data_ptr(),
+        t1.data_ptr(), t2.data_ptr(), t3.data_ptr(), ctypes.c_void_p(stream)), "wds_adjoint")
+    cnt = torch.bincount(b_idx, minlength=B)
+    cmax = int(cnt.max())
+    first = torch.cumsum(cnt, 0) - cnt
+    j_idx = torch.arange(b_idx.numel(), device=dev) - first[b_idx]
+    n1 = torch.as_tensor(s._n1, device=dev)[k_idx]
+    n2 = torch.as_tensor(s._n2, device=dev)[k_idx]
+    junc = torch.as_tensor(s._tables["node_type"] == 0, device=dev)
+    m1 = junc[n1].to(torch.float64)
+    m2 = junc[n2].to(torch.float64)
+    # columns x_c = M^{-1} a_c, rows b * cmax + j of wds_adjoint_rhs (gH = -a_c)
+    R = B * cmax
+    X = torch.empty(R, N, dtype=torch.float64, device=dev)
+    v = b_idx * cmax + j_idx
+    cap = plan.max_batch
+    for v0 in range(0, R, cap):
+        nb = min(cap, R - v0)
+        gHx = torch.zeros(nb, N, dtype=torch.float64, device=dev)
+        sel = (v >= v0) & (v < v0 + nb)
+        vv = v[sel] - v0
+        gHx.index_put_((vv, n1[sel]), -m1[sel], accumulate=True)
+        gHx.index_put_((vv, n2[sel]), m2[sel], accumulate=True)
+        z0 = torch.zeros(nb, L, dtype=torch.float64, device=dev)
+        zN = torch.zeros(nb, N, dtype=torch.float64, device=dev)
+        o1, o2 = torch.empty_like(zN), torch.empty_like(zN)
+        o3 = torch.empty_like(z0)
+        _lib.check(plan.lib.wds_adjoint_rhs(
+            plan.handle, nb, cmax, v0, gHx.data_ptr(), z0.data_ptr(), zN.data_ptr(),
+            X[v0:v0 + nb].data_ptr(), o1.data_ptr(), o2.data_ptr(), o3.data_ptr(),
+            ctypes.c_void_p(stream)), "wds_adjoint_rhs")
+    Xr = X.view(B, cmax, N)
+    # G[b, i, j] = a_i^T x_j; padded entries get a unit diagonal and a zero rhs
+    G = torch.zeros(B, cmax, cmax, dtype=torch.float64, device=dev)
+    G[b_idx, j_idx, :] = Xr[b_idx, :, n1] * m1[:, None] - Xr[b_idx, :, n2] * m2[:, None]
+    dg = torch.ones(B, cmax, dtype=torch.float64, device=dev)
+    dg[b_idx, j_idx] = 1.0 / dP
+    rhs = torch.zeros(B, cmax, dtype=torch.float64, device=dev)
+    rhs[b_idx, j_idx] = lam[b_idx, n1] * m1 - lam[b_idx, n2] * m2
+    z = torch.linalg.solve(G + torch.diag_embed(dg), rhs.unsqueeze(-1)).squeeze(-1)
+    zc = z[b_idx, j_idx]
+    gH2 = gH.clone()
+    gH2.index_put_((b_idx, n1), zc * m1, accumulate=True)
+    gH2.index_put_((b_idx, n2), -zc * m2, accumulate=True)
+    return gH2, (b_idx, k_idx, dP, n1, n2, m1, m2)
+
+
+def _clamp_grh(fix, gQ, gd, grh):
+    """The clamped pump's own link adjoint lambda_l = P (gQ - (l2 - l1)) enters
+    the reservoir-head gradient at a fixed endpoint; the adjoint launch formed
+    it with the assembled P, so add dP (gQ - (l2 - l1)) there (+ at n1, - at
+    n2, dgga/autodiff.py:726-732)."""
+    b_idx, k_idx, dP, n1, n2, m1, m2 = fix
+    l1 = gd[b_idx, n1] * m1
+    l2 = gd[b_idx, n2] * m2
+    corr = dP * (gQ[b_idx, k_idx] - (l2 - l1))
+    grh.index_put_((b_idx, n1), corr * (1.0 - m1), accumulate=True)
+    grh.index_put_((b_idx, n2), -corr * (1.0 - m2), accumulate=True)
 
 
 class ImplicitGGASolveSM100(torch.autograd.Function):
@@ -108,7 +206,7 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
             raise RuntimeError(
                 "adjoint='gpu': scenarios %s did not converge (relerr=%s > accuracy=%g)"
                 % (bad[:8], [float(o["relerr"][b]) for b in bad[:4]], float(accuracy)))
-        _adjoint_guards(s, o["flow"], o["status"], pumps)
+        ctx.clamp = _adjoint_guards(s, o["flow"], o["status"], pumps, allow_clamp=True)
         ctx.solver = s
         ctx.pumps = pumps      # keeps the rows alive with the kept state
         ctx.th = tuple(None if x is None else (x.dim(), x.device) for x in th_in)
@@ -147,6 +245,9 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         p = ctx.plan
         cur = torch.cuda.current_stream(dev)
         ev = s._event_pair(cur, "adjoint")
+        fix = None
+        if ctx.clamp is not None:
+            gH, fix = _clamp_rhs(s, p, B, ctx.clamp, gH, gQ, gE, cur.cuda_stream)
         want_th = any(x is not None for x in ctx.th) and any(ctx.needs_input_grad[9:12])
         if want_th:
             gth = torch.empty(3, B, L, dtype=torch.float64, device=dev)
@@ -160,6 +261,8 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
                 p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
                 grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
                 "wds_adjoint")
+        if fix is not None:
+            _clamp_grh(fix, gQ, gd, grh)
         if ev is not None:
             ev[1].record(cur)
         dm, dv = ctx.dims, ctx.devs

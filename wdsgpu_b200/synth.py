@@ -529,6 +529,30 @@ def eps_demands(net, T, B, seed=0, sigma=0.15, t0_hours=0.0):
     return d0[None, None, :] * m[:, None, None] * noise
 
 
+def chp_dead_end_network(demand_cfs=2e-4, seed=5):
+    """The feature network with its constant-horsepower pump re-routed to
+    feed a new dead-end junction of tiny demand: at convergence the pump
+    carries only that demand, and its gradient -r/q^2 lies above CBIG (the
+    clamp branch hloss = -CBIG q of hydcoeffs.c:748-752)."""
+    net = feature_network(seed=seed, with_chp=True)
+    k = int(net.pump_link[3])
+    n1 = int(net.link_n1[k])
+    x = net.N
+    f = net.as_fields()
+    f["node_id"] = list(net.node_id) + ["CHPX"]
+    f["node_type"] = np.append(net.node_type, np.int8(JUNCTION)).astype(np.int8)
+    f["elev_ft"] = np.append(net.elev_ft, net.elev_ft[n1])
+    f["node_ke"] = np.append(net.node_ke, 0.0)
+    f["res_head_pat"] = np.append(net.res_head_pat, -1).astype(np.int32)
+    n2 = np.asarray(net.link_n2).copy()
+    n2[k] = x
+    f["link_n2"] = n2.astype(np.int32)
+    f["dem_node"] = np.append(net.dem_node, x).astype(np.int32)
+    f["dem_base_cfs"] = np.append(net.dem_base_cfs, demand_cfs)
+    f["dem_pat"] = np.append(net.dem_pat, -1).astype(np.int32)
+    return Net(**f)
+
+
 def config5_network(seed=5, tank_center_ft=None):
     """Extended-period workload shape: about 20 000 junctions and 23 000
     pipes, 4 power-function pumps (shutoff 40-60 m, exponent 1.85),
