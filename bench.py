@@ -45,10 +45,13 @@ POLISH = 3
 ACCURACY = 1e-6
 
 
-def bytes_per_iteration(L, nA, nL, Nj, w=8):
-    """Streaming model of one Newton iteration (coefficients, assembly, LDL^T,
-    solve + 2 refinements, update): 64 L + (24 + w) nA + 7 w nL + 96 Nj."""
-    return 64 * L + (24 + w) * nA + 7 * w * nL + 96 * Nj
+def bytes_per_iteration(L, nA, nL, Nj, w=8, refine=2):
+    """Streaming model of one Newton iteration: coefficients 24 L, assembly
+    8 L + 8 nA + 8 Nj, LDL^T w (nA + nL), solve 2 w nL + 16 Nj, each
+    refinement 8 nA + 2 w nL + 32 Nj, update 8 Nj + 32 L; with 2 refinements
+    64 L + (24 + w) nA + 7 w nL + 96 Nj."""
+    return (64 * L + (8 + w + 8 * refine) * nA + (3 + 2 * refine) * w * nL
+            + (32 + 32 * refine) * Nj)
 
 
 def adjoint_bytes(L, N, nA, nL, Nj, w=8):
@@ -439,9 +442,13 @@ def main():
     st = s.plan_stats(B)
     iters = s.run(d_dev, rh_dev, ke_dev.unsqueeze(0), r_dev.unsqueeze(0), B, 200, ACCURACY,
                   True, POLISH)["iters"].double()
-    n_fac = float((iters + POLISH + 1).sum())
-    bpi = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"])
-    fwd_bytes = n_fac * bpi
+    # GGA iterations counted without refinement (the band refines only the
+    # last one or two of them, so this is a lower bound); polish steps and
+    # the terminal factor with two refinements
+    rg = s.refine_steps() if s.refine_band(ACCURACY) <= 0.0 else 0
+    bpi = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"], refine=rg)
+    bpi2 = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"])
+    fwd_bytes = float(iters.sum()) * bpi + B * (POLISH + 1) * bpi2
     fwd_avg_ms = statistics.mean(fwd_ms) if fwd_ms else float("nan")
     adj_avg_ms = statistics.mean(adj_ms) if adj_ms else float("nan")
     dominant = "k_forward" if fwd_avg_ms >= adj_avg_ms else "k_adjoint"
@@ -471,7 +478,9 @@ def main():
                          "peak_source": peak_kind,
                          "traffic": (traffic_per_scen * B if traffic_per_scen else None),
                          "algorithmic_bytes": fwd_bytes,
-                         "model": "bytes/iter = 64L + 32 nA + 56 nL + 96 Nj = %d B; x (iters+%d) per scenario" % (bpi, POLISH + 1)},
+                         "model": "bytes/iter = 64L + (16+8r) nA + (3+2r) 8 nL + (32+32r) Nj, r refinements: "
+                                  "%d B at r=%d x GGA iters + %d B at r=2 x %d (polish + terminal) per scenario"
+                                  % (bpi, rg, bpi2, POLISH + 1)},
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline and world == 1:

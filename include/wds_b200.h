@@ -133,7 +133,7 @@ typedef struct WdsForwardOpts {
   double accuracy;               /* hacc (relerr threshold)                  */
   int32_t max_iter;              /* trials                                   */
   int32_t status_machine;        /* 1: batched status machine                */
-  int32_t refine;                /* refinement steps per linear solve (2)    */
+  int32_t refine;                /* refinement steps per linear solve (2); see refine_band */
   int32_t polish_steps;          /* reduced Newton polish steps; <0: plain solve only */
   int64_t ke_stride;             /* row stride of ke (0: one row for all)    */
   int64_t r_stride;              /* row stride of r  (0: one row for all)    */
@@ -150,6 +150,17 @@ typedef struct WdsForwardOpts {
   const double* pump_h0;         /* curve coefficient H0                    */
   const double* pump_r;          /* curve coefficient R                     */
   int64_t pump_stride;
+  /* Which GGA iterations refine their solve (dense_refine / cudss_refine of
+   * the reference refine every one, dgga/solver.py:3056, 2647).  0: every
+   * iteration.  > 0: an iteration refines when the previous iteration's
+   * relerr is below refine_band (or past iteration 20); the others take one
+   * unrefined FP64 substitution.  While relerr is far above the rounding an
+   * unrefined solve adds (about 1e-11 to 1e-9 relative), the Newton
+   * iteration corrects that rounding by itself.  GGASolver passes 1e-5 at
+   * accuracy >= 1e-8 (where that rounding is also far below the convergence
+   * test) and 0 at tighter accuracies.  Polish and adjoint solves always
+   * refine. */
+  double refine_band;
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;

@@ -48,7 +48,8 @@ def test_noalloc_forward_matches_wds_forward_on_two_calls(cuda):
     rh = torch.tensor(rh_np, device=cuda)
     ke = s.node_ke_default.unsqueeze(0).contiguous()
     r = s.r_hw.unsqueeze(0).contiguous()
-    ref = s.run(d, rh, ke, r, B, 200, 1e-6, True, 3)       # wds_forward, plan workspace
+    ref = s.run(d, rh, ke, r, B, 200, 1e-6, True, 3, refine=2,   # wds_forward, same options
+                refine_band=0.0)
     plan = ref["plan"]
     lib = _lib.load()
     opts = _lib.WdsForwardOpts()

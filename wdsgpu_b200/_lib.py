@@ -65,6 +65,7 @@ class WdsForwardOpts(ctypes.Structure):
         ("r_stride", ctypes.c_int64), ("q0", ctypes.c_void_p), ("e0", ctypes.c_void_p),
         ("pump_speed", ctypes.c_void_p), ("pump_h0", ctypes.c_void_p),
         ("pump_r", ctypes.c_void_p), ("pump_stride", ctypes.c_int64),
+        ("refine_band", ctypes.c_double),
     ]
 
 

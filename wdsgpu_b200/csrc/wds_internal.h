@@ -133,6 +133,7 @@ struct FwdArgs {
   int B;
   double hacc;
   int max_iter, sm, refine, polish;
+  double rband;  // refine a GGA solve only when the previous relerr < rband (0: always)
   long long ke_stride, r_stride;
   const double* d;
   const double* rh;

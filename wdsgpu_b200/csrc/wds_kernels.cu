@@ -969,12 +969,12 @@ __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const
 template <int NT, class FT, class TB>
 __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
-                             bool any_act, int refine) {
+                             bool any_act) {
   const double* rhs = s.V0;
   double* t = s.V2;
   const int tid = gtid<NT>();
-  if (!any_act) {
-    solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, refine);
+  if (!any_act) {  // two refinement steps, as the reference's polish solves
+    solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, 2);
     return;
   }
   const int p = n.npcv, m = 2 * p;
@@ -1228,7 +1228,10 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
       iters = it;
       break;
     }
-    solve_refined<NT, FT>(n, T, s, s.V0, -1, s.V1, s.V2, a.refine);
+    // refinement only where it can matter for the convergence test (see
+    // WdsForwardOpts.refine_band); relerr still holds the previous iteration's
+    const bool refine_it = a.rband <= 0.0 || it > 20 || (it > 1 && relerr < a.rband);
+    solve_refined<NT, FT>(n, T, s, s.V0, -1, s.V1, s.V2, refine_it ? a.refine : 0);
     // ---- newflows (hydsolver.c:358-514 as restated in solver.py:3092-3110)
     double sums[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k = gtid<NT>(); k < n.L; k += NT) {
@@ -1401,7 +1404,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
         s.V0[p] = (mm - bt) + emh * re;
       }
       gsync<NT>();
-      primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act, a.refine);
+      primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act);
       // dq, de, state update
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);

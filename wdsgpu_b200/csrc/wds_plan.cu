@@ -742,9 +742,13 @@ extern "C" int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* co
 }
 
 namespace wds {
-// Pump parameters of a forward call: rows of [L] at stride 0 (one row for all
-// scenarios) or L (one per scenario).
+// Options of a forward call beyond the basic ones: pump parameters (rows of
+// [L] at stride 0, one row for all scenarios, or L, one per scenario) and the
+// refinement band of the GGA iterations.
 static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::string& who) {
+  if (!(o->refine_band >= 0.0))
+    return fail(WDS_E_ARG, who + ": refine_band must be >= 0");
+  a.rband = o->refine_band;
   a.th_sp = o->pump_speed;
   a.th_h0 = o->pump_h0;
   a.th_r = o->pump_r;

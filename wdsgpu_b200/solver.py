@@ -147,7 +147,16 @@ class GGASolver:
     with a setting must join two junctions.
 
     `sm100_refine` (default 2) is the number of iterative-refinement steps of
-    every linear solve, mirroring `dense_refine` / `cudss_refine`.
+    a refined GGA solve, mirroring `dense_refine` / `cudss_refine`.
+    `sm100_refine_band` says which GGA iterations refine: an iteration whose
+    previous relerr is below the band (or past iteration 20) refines, the
+    others take one unrefined FP64 substitution, whose rounding (about 1e-11
+    to 1e-9 relative) the Newton iteration corrects by itself while relerr
+    is far above it.  None (default): 1e-5 with the FP64 factor at
+    accuracy >= 1e-8, where that rounding is far below the convergence test
+    as well; 0 (every iteration, the reference's schedule) at tighter
+    accuracies and with the FP32 factor.  Polish and adjoint solves always
+    refine.
     `sm100_layout` ("auto", "shared" or "global", set before the first solve)
     says where the schedule tables and per-scenario state live: shared memory
     (several scenarios per SM), or global memory for networks too large for
@@ -178,6 +187,7 @@ class GGASolver:
         self.dtype = dtype
         self.net = net
         self.sm100_refine = 2
+        self.sm100_refine_band = None
         self.sm100_layout = "auto"
         self.sm100_factor_dtype = torch.float64
         # emitters per scenario kept in shared memory (junctions with Ke > 0)
@@ -496,6 +506,18 @@ class GGASolver:
         if record_schedule:
             raise NotImplementedError("record_schedule is not provided by the sm100 route")
 
+    def refine_steps(self):
+        """Refinement steps of a refined GGA solve (`sm100_refine`)."""
+        return int(self.sm100_refine)
+
+    def refine_band(self, accuracy):
+        """Refinement band of the GGA iterations (see `sm100_refine_band`)."""
+        if self.sm100_refine_band is not None:
+            return float(self.sm100_refine_band)
+        if self.sm100_factor_dtype == torch.float32 or float(accuracy) < 1e-8:
+            return 0.0
+        return 1e-5
+
     def pump_rows(self, B, speed=None, pump_h0=None, pump_r=None):
         """Pump parameters of a call as FP64 device rows: (speed, h0, r), each
         None or [1, L] / [B, L] with one common row count (an [L] row next to
@@ -533,7 +555,7 @@ class GGASolver:
         return tuple(None if t is None else t.expand(rows, L).contiguous() for t in out)
 
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
-            refine=None, plan=None, q0=None, e0=None, pumps=None):
+            refine=None, plan=None, q0=None, e0=None, pumps=None, refine_band=None):
         """One wds_forward call on device tensors; returns the raw outputs.
         q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
         warm start of GGASolver.solve (dgga/solver.py:2876-2887); pumps is
@@ -552,7 +574,8 @@ class GGASolver:
         o.accuracy = float(hacc)
         o.max_iter = int(max_iter)
         o.status_machine = 1 if status_machine else 0
-        o.refine = int(self.sm100_refine if refine is None else refine)
+        o.refine = int(self.refine_steps() if refine is None else refine)
+        o.refine_band = float(self.refine_band(hacc) if refine_band is None else refine_band)
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
