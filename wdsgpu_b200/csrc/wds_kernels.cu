@@ -551,20 +551,24 @@ __device__ __forceinline__ void bwd_level(const TB& T, const FT* W, double* v, i
 
 // Inverse of the top block's Schur complement S (nT x nT, nT <= WDS_TOP_MAX)
 // by symmetric sweeps (Gauss-Jordan elimination without pivoting, in column
-// order; its pivots are the LDL^T pivots of S, positive for an SPD matrix):
+// order; every pivot is then a pivot of the LDL^T of S, so its sign is the
+// positive-definiteness check):
 // sweeping k maps a_kk -> -1/p, a_ik -> a_ik/p, a_kj -> a_kj/p and
 // a_ij -> a_ij - (a_ik/p) a_kj (p = a_kk); after all nT sweeps the matrix is
-// -S^{-1}.  The matrix stays symmetric, so only its lower triangle is kept:
-// thread (r, c) of a 16 x 16 grid holds entries (r + 16 a, c + 16 b),
-// b <= a < 3, in registers for all sweeps.  Column k+1 after sweep k goes
-// through shared memory: two alternating buffers of 49 (the column, zero
-// beyond nT, then 1/p of its pivot, which the pivot's owner computes and
-// checks); one group barrier per sweep.  Every entry takes the general update
-// without a test; the few lanes owning row or column k then overwrite those
-// entries.  S is read from the factor slots listed in dslot, S^{-1} is
-// written to Mg (row-major, both triangles).  Returns 1 when this thread
-// owned a pivot that was not positive and finite.  Runs as a separate
-// function so that its block of registers does not add to the caller's.
+// -S^{-1}.  Thread (r, c) of a 16 x 16 grid holds the entries
+// (r + 16 a, c + 16 b), a, b < 3, of the full matrix in registers for all
+// sweeps, so that a sweep is one short run of instructions per thread (the
+// rank-1 update is 9 FMAs; the sweeps are issue-bound when the SM's scenario
+// groups overlap).  Column k+1 after sweep k goes through shared memory: two
+// alternating buffers of 49 (the column, zero beyond nT, then 1/p of its
+// pivot, which the pivot's owner computes and checks) and one group barrier
+// per sweep.  Every entry takes the general update; the lanes owning column
+// k, then those owning row k, overwrite those entries (switches on the
+// uniform block index, so the registers are never indexed at run time).  S is
+// read from the factor slots listed in dslot, S^{-1} is written to Mg
+// (row-major, each entry by its owner).  Returns 1 when this thread owned a
+// pivot that was not positive and finite.  Runs as a separate function so
+// that its block of registers does not add to the caller's.
 template <int NT, class Slot, class FT>
 __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* tb,
                                         double* Mg, int nT) {
@@ -576,14 +580,15 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
 #pragma unroll
   for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-    for (int ib = 0; ib <= ia; ++ib) {
-      const int i = r + 16 * ia, j = c + 16 * ib;
+    for (int jb = 0; jb < 3; ++jb) {
+      const int i = r + 16 * ia, j = c + 16 * jb;
       double x = 0.0;
-      if (i < nT && j <= i) {
-        const Slot sl = dslot[i * (i + 1) / 2 + j];
+      if (i < nT && j < nT) {
+        const int hi = i > j ? i : j, lo = i > j ? j : i;
+        const Slot sl = dslot[hi * (hi + 1) / 2 + lo];
         if (sl != (Slot)~Slot(0)) x = (double)W[sl];
       }
-      a[ia][ib] = x;
+      a[ia][jb] = x;
     }
   // both buffers zero (rows beyond nT stay zero), then column 0 and 1/p of its pivot
   if (tid < 2 * ST) tb[tid] = 0.0;
@@ -604,51 +609,42 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
     double* nb = tb + ((k + 1) & 1) * ST;
     const double ip = cb[WDS_TOP_MAX];
     const double c0 = cb[c], c1 = cb[c + 16], c2 = cb[c + 32];
-    const double t0 = cb[r] * ip, t1 = cb[r + 16] * ip, t2 = cb[r + 32] * ip;
-    a[0][0] = fma(-t0, c0, a[0][0]);
-    a[1][0] = fma(-t1, c0, a[1][0]);
-    a[1][1] = fma(-t1, c1, a[1][1]);
-    a[2][0] = fma(-t2, c0, a[2][0]);
-    a[2][1] = fma(-t2, c1, a[2][1]);
-    a[2][2] = fma(-t2, c2, a[2][2]);
     const int km = k & 15, kb = k >> 4;
-    if (r == km || c == km) {  // entries in row k or column k
-      const double ti[3] = {t0, t1, t2}, cj[3] = {c0, c1, c2};
+    // general update; column k (a_ik = a_ik / p) where this lane owns it
+    const bool k0 = c == km && kb == 0, k1 = c == km && kb == 1, k2 = c == km && kb == 2;
 #pragma unroll
-      for (int ia = 0; ia < 3; ++ia)
-#pragma unroll
-        for (int ib = 0; ib <= ia; ++ib) {
-          const bool ri = r == km && ia == kb, cj_ = c == km && ib == kb;
-          if (ri && cj_) a[ia][ib] = -ip;
-          else if (ri) a[ia][ib] = cj[ib] * ip;
-          else if (cj_) a[ia][ib] = ti[ia];
-        }
+    for (int ia = 0; ia < 3; ++ia) {
+      const double t = cb[r + 16 * ia] * ip;
+      a[ia][0] = k0 ? t : fma(-t, c0, a[ia][0]);
+      a[ia][1] = k1 ? t : fma(-t, c1, a[ia][1]);
+      a[ia][2] = k2 ? t : fma(-t, c2, a[ia][2]);
     }
-    // publish column kn = k + 1: rows i >= kn from the owners of column kn,
-    // rows i < kn from the owners of row kn (a_{i,kn} = a_{kn,i})
-    const int kn = k + 1;
-    if (kn < nT) {
-      const int nm = kn & 15, nbk = kn >> 4;
-      if (c == nm) {
-#pragma unroll
-        for (int ia = 0; ia < 3; ++ia) {
-          const int i = r + 16 * ia;
-          if (ia >= nbk && i >= kn) {
-            const double x = nbk == 0 ? a[ia][0] : nbk == 1 ? a[ia][1] : a[ia][2];
-            nb[i] = x;
-            if (i == kn) {
-              if (!(x > 0.0) || !isfinite(x)) bad = 1;
-              nb[WDS_TOP_MAX] = __drcp_rn(x);
-            }
-          }
-        }
+    if (r == km) {  // row k: a_kj = a_kj / p, and a_kk = -1/p
+      const double r0 = k0 ? -ip : c0 * ip;
+      const double r1 = k1 ? -ip : c1 * ip;
+      const double r2 = k2 ? -ip : c2 * ip;
+      if (kb == 0) {
+        a[0][0] = r0; a[0][1] = r1; a[0][2] = r2;
+      } else if (kb == 1) {
+        a[1][0] = r0; a[1][1] = r1; a[1][2] = r2;
+      } else {
+        a[2][0] = r0; a[2][1] = r1; a[2][2] = r2;
       }
-      if (r == nm) {
-#pragma unroll
-        for (int ib = 0; ib < 3; ++ib) {
-          const int j = c + 16 * ib;
-          if (ib <= nbk && j < kn) nb[j] = nbk == 0 ? a[0][ib] : nbk == 1 ? a[1][ib] : a[2][ib];
-        }
+    }
+    // publish column kn = k + 1 (all rows: the full matrix is kept) and 1/p
+    const int kn = k + 1;
+    if (kn < nT && c == (kn & 15)) {
+      const int nj = kn >> 4;
+      const double v0 = nj == 0 ? a[0][0] : (nj == 1 ? a[0][1] : a[0][2]);
+      const double v1 = nj == 0 ? a[1][0] : (nj == 1 ? a[1][1] : a[1][2]);
+      const double v2 = nj == 0 ? a[2][0] : (nj == 1 ? a[2][1] : a[2][2]);
+      nb[r] = v0;
+      nb[r + 16] = v1;
+      nb[r + 32] = v2;
+      if (r == (kn & 15)) {
+        const double x = nj == 0 ? v0 : (nj == 1 ? v1 : v2);
+        if (!(x > 0.0) || !isfinite(x)) bad = 1;
+        nb[WDS_TOP_MAX] = __drcp_rn(x);
       }
     }
     gsync<NT>();
@@ -656,18 +652,13 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
 #pragma unroll
   for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-    for (int ib = 0; ib <= ia; ++ib) {
-      const int i = r + 16 * ia, j = c + 16 * ib;
-      if (i < nT && j <= i) {
-        Mg[i * nT + j] = -a[ia][ib];
-        Mg[j * nT + i] = -a[ia][ib];
-      }
+    for (int jb = 0; jb < 3; ++jb) {
+      const int i = r + 16 * ia, j = c + 16 * jb;
+      if (i < nT && j < nT) Mg[i * nT + j] = -a[ia][jb];
     }
   return bad;
 }
 
-// x_T = S^{-1} r_T for the top rows of v (vT = v + cT): row i of the product
-// on 4 lanes, each summing 12 or fewer terms; ends with a group barrier.
 template <int NT>
 __device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
   const int tid = gtid<NT>(), i = tid >> 2, li = tid & 3;
