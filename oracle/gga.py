@@ -216,6 +216,20 @@ class Model:
         self.prv_j1, self.prv_j2 = jrow[self.prv_n1], jrow[self.prv_n2]
         self.prv_hset = self.el[self.prv_n2] + K0[self.pcv]
         self.prv_km = self.km[self.pcv]
+        # FCVs with a flow setting (fcvcoeff / fcvstatus of the EPANET replica,
+        # solver.py:1665-1695, 1816-1826, 1875-1877); fixed ones are fixed valves
+        fcv = np.flatnonzero(lt == _FCV)
+        self.fcv = fcv[K0[fcv] != MISSING]
+        self.prv_fixed[fcv[K0[fcv] == MISSING]] = True
+        self.fcv_mask = np.zeros(L, dtype=bool)
+        self.fcv_mask[self.fcv] = True
+        self.fcv_j1, self.fcv_j2 = jrow[n1[self.fcv]], jrow[n2[self.fcv]]
+        self.fcv_qs = K0[self.fcv]
+        self.fcv_km = self.km[self.fcv]
+        self.vmask = self.pcv_mask | self.fcv_mask
+        # valvecoeffs visit the valves in link order (hydcoeffs.c:282-330)
+        self.vorder = sorted([(int(k), 0, i) for i, k in enumerate(self.pcv)]
+                             + [(int(k), 1, j) for j, k in enumerate(self.fcv)])
 
     # ---------------------------------------------------------------- coeffs
     def pipe_PY(self, q, r):
@@ -393,20 +407,57 @@ class Model:
             Pv, Yv = self._valve_open(q, self.km)
             P, Y = np.where(self.prv_fixed, Pv, P), np.where(self.prv_fixed, Yv, Y)
         closed = ((S <= CLOSED) | self.zero_speed) if S is not None else self.closed_dense
-        if self.pcv.size:
-            closed = closed & ~self.pcv_mask
+        if self.vmask.any():
+            closed = closed & ~self.vmask
         P = np.where(closed, 1.0 / CBIG, P)
         Y = np.where(closed, q, Y)
-        if self.pcv.size:
-            P = np.where(self.pcv_mask, 0.0, P)
-            Y = np.where(self.pcv_mask, 0.0, Y)
+        if self.vmask.any():
+            P = np.where(self.vmask, 0.0, P)
+            Y = np.where(self.vmask, 0.0, Y)
         return P, Y, closed
 
-    def prv_coeffs(self, P, Y, F, A, Xflow, q, S):
-        """Batched PRV valve coefficients after nodecoeffs (solver.py:850-912).
-        A is the dense [B,Nj*Nj] matrix (or None)."""
+    def _fcv_coeffs(self, j, P, Y, F, A, Xflow, q, S):
+        """One FCV in the valve pass (fcvcoeff, solver.py:1665-1695): ACTIVE
+        cuts the network (an outflow qset at n1, an inflow at n2, P = 1/CBIG,
+        Y = q - qset); otherwise the open / closed valve coefficients."""
         Nj = self.Nj
-        for i, k in enumerate(self.pcv):
+        k, j1, j2, qs = self.fcv[j], self.fcv_j1[j], self.fcv_j2[j], self.fcv_qs[j]
+        qk, sk = q[:, k], S[:, k]
+        act = sk == ACTIVE
+        cl = sk <= CLOSED
+        km = self.fcv_km[j]
+        if km > 0.0:
+            hg = 2.0 * km * np.abs(qk)
+            lin = hg < self.rqtol
+            hg = np.where(lin, self.rqtol, hg)
+            hl = np.where(lin, qk * hg, qk * hg / 2.0)
+            po, yo = 1.0 / hg, hl / hg
+        else:
+            po, yo = np.full_like(qk, 1.0 / CSMALL), qk
+        pv, yv = np.where(cl, 1.0 / CBIG, po), np.where(cl, qk, yo)
+        pk = np.where(act, 1.0 / CBIG, pv)
+        yk = np.where(act, qk - qs, yv)
+        Xflow[:, j1] -= qs * act
+        Xflow[:, j2] += qs * act
+        F[:, j1] += np.where(act, -qs, yv - qk)
+        F[:, j2] += np.where(act, qs, -(yv - qk))
+        if A is not None:
+            for slot, v in ((j1 * Nj + j2, -pk), (j2 * Nj + j1, -pk),
+                            (j1 * Nj + j1, pk), (j2 * Nj + j2, pk)):
+                A[:, slot] += v
+        P[:, k] = pk
+        Y[:, k] = yk
+
+    def prv_coeffs(self, P, Y, F, A, Xflow, q, S):
+        """Batched valve coefficients after nodecoeffs, in valve (link) order:
+        PRVs as solver.py:850-912, FCVs as `_fcv_coeffs`.  A is the dense
+        [B,Nj*Nj] matrix (or None)."""
+        Nj = self.Nj
+        for _, kind, i in self.vorder:
+            if kind == 1:
+                self._fcv_coeffs(i, P, Y, F, A, Xflow, q, S)
+                continue
+            k = self.pcv[i]
             j1, j2 = self.prv_j1[i], self.prv_j2[i]
             qk, sk = q[:, k], S[:, k]
             act, cl = sk == ACTIVE, sk <= CLOSED
@@ -458,6 +509,12 @@ class Model:
         if self.n_pumps:
             xh = np.where(-dh > self.pump_hmax_sm + self.htol, XHEAD, OPEN)
             s = np.where(self.pump_live & (s >= OPEN), xh, s).astype(np.int8)
+        if self.fcv.size:   # fcvstatus from the status before the reopening
+            kf = self.fcv
+            qk, s0 = q[:, kf], st0[:, kf]
+            rev = (dh[:, kf] < -self.htol) | (qk < -self.qtol)
+            s[:, kf] = np.where(rev, XFCV, np.where((s0 == XFCV) & (qk >= self.fcv_qs),
+                                                    ACTIVE, s0))
         k = self.tl_k
         if k.size:
             live = s[:, k] > CLOSED
@@ -526,7 +583,7 @@ class Model:
         Xf = Xf - em * e
         Xf = Xf - d
         F = F + Xf
-        if self.pcv.size:
+        if self.vmask.any():
             P, Y, F, A = self.prv_coeffs(P.copy(), Y.copy(), F, A, Xf, q, S)
         return P, Y, F, A.reshape(B, Nj, Nj), hle, hge, em
 
@@ -578,8 +635,8 @@ class Model:
             S = np.broadcast_to(self.S0, (B, self.L)).copy()
             maxtrials = max_iter + (self.extra_iter if self.extra_iter > 0 else 0)
             nextcheck = np.full(B, self.checkfreq, dtype=np.int64)
-        elif self.pcv.size or self.is_cv.any():
-            raise NotImplementedError("PRV/CV networks need status_machine=True")
+        elif self.vmask.any() or self.is_cv.any():
+            raise NotImplementedError("PRV/FCV/CV networks need status_machine=True")
         for it in range(1, maxtrials + 1):
             P, Y, _ = self.headloss_PY(q, r, S)
             P, Y, F, A, hle, hge, em = self._assemble(P, Y, q, H, e, ke_j, d_j, S)
@@ -638,14 +695,15 @@ class Model:
         """Coefficients at the current state (autodiff.py:786-875)."""
         P, Y, closed = self.headloss_PY(q, r, S)
         act = None
-        if self.pcv.size:
+        if self.vmask.any():
             B = q.shape[0]
             Yd = np.zeros_like(q)
             P, Y2, _, _ = self.prv_coeffs(P.copy(), Yd, np.zeros((B, self.Nj)), None,
                                           np.zeros((B, self.Nj)), q, S)
             Y = Y.copy()
-            Y[:, self.pcv] = Y2[:, self.pcv]
-            act = S[:, self.pcv] == ACTIVE
+            Y[:, self.vmask] = Y2[:, self.vmask]
+            if self.pcv.size:
+                act = S[:, self.pcv] == ACTIVE
         _, hge = self.emitter(e, ke)
         em = (ke > 0.0).astype(float)
         emh = em / hge

@@ -9,7 +9,7 @@ import torch
 
 from wdsgpu_b200 import synth
 from wdsgpu_b200.autodiff import dr_dC, hw_resistance, implicit_solve
-from wdsgpu_b200.net import FCV, PSV
+from wdsgpu_b200.net import FCV, PBV, PSV
 from wdsgpu_b200.solver import GGASolver
 
 
@@ -22,9 +22,13 @@ def test_unsupported_link_types_raise():
     n2.link_type[0] = PSV
     with pytest.raises(NotImplementedError):
         GGASolver(n2, device="cpu", dense_status_machine=True)
-    n2.link_type[0] = FCV
+    n2.link_type[0] = PBV
     with pytest.raises(NotImplementedError):
         GGASolver(n2, device="cpu", dense_status_machine=True)
+    n2.link_type[0] = FCV                          # batched FCVs (status machine only)
+    GGASolver(n2, device="cpu", dense_status_machine=True)
+    with pytest.raises(NotImplementedError):
+        GGASolver(n2, device="cpu", dense_status_machine=False)
 
 
 def test_meta_guards():

@@ -83,6 +83,19 @@ struct DevNet {
   const int* pcv_xf;      // Xflow slot of j2
   const double* pcv_hset;
   const double* pcv_km;
+  // status-machine FCVs [nfcv] (valve pass and fcvstatus; never constraint rows)
+  int nfcv;
+  const int* link_fcv;    // [L] fcv index or -1
+  const int* fcv_link;
+  const int* fcv_j1;
+  const int* fcv_j2;
+  const int* fcv_off;     // factor slot of the (j1, j2) entry
+  const int* fcv_xf1;     // Xflow slots of its ends read by later PRVs, or -1
+  const int* fcv_xf2;
+  const double* fcv_qs;   // flow setting (cfs)
+  const double* fcv_km;
+  // valve pass order [npcv + nfcv]: link order; v >= 0 PRV v, v < 0 FCV -1 - v
+  const int* vord;
   // tank links [ntl]
   const int* tl_link;
   const int* tl_tank;     // fixed index

@@ -313,12 +313,12 @@ __device__ void pump_coef(const DevNet& n, const PumpTh& th, int k, double q, do
   Y = hl / hg;
 }
 
-// PRV valve coefficients of one status-machine PRV (dgga/solver.py:862-903):
-// returns pna (the non-ACTIVE P, zero when ACTIVE) and yna.
-__device__ __forceinline__ void prv_open(const DevNet& n, int i, double qk, int sk, double& pna,
-                                         double& yna) {
-  const bool act = sk == WDS_ACTIVE, cl = sk <= WDS_CLOSED;
-  const double km = n.pcv_km[i];
+// Coefficients of a control valve that is not ACTIVE (valvecoeff, as
+// restated in dgga/solver.py:862-903 and _valvecoeff_scalar): CLOSED is the
+// 1/CBIG branch, otherwise the minor-loss Km (or 1/CSMALL for Km = 0).
+__device__ __forceinline__ void valve_state_coef(const DevNet& n, double km, double qk, int sk,
+                                                 double& P, double& Y) {
+  const bool cl = sk <= WDS_CLOSED;
   double po, yo;
   if (km > 0.0) {
     double hg = 2.0 * km * fabs(qk);
@@ -331,8 +331,17 @@ __device__ __forceinline__ void prv_open(const DevNet& n, int i, double qk, int 
     po = 1.0 / kCSMALL;
     yo = qk;
   }
-  pna = (cl ? 1.0 / kCBIG : po) * (act ? 0.0 : 1.0);
-  yna = cl ? qk : yo;
+  P = cl ? 1.0 / kCBIG : po;
+  Y = cl ? qk : yo;
+}
+
+// PRV valve coefficients of one status-machine PRV (dgga/solver.py:862-903):
+// returns pna (the non-ACTIVE P, zero when ACTIVE) and yna.
+__device__ __forceinline__ void prv_open(const DevNet& n, int i, double qk, int sk, double& pna,
+                                         double& yna) {
+  double P;
+  valve_state_coef(n, n.pcv_km[i], qk, sk, P, yna);
+  pna = P * (sk == WDS_ACTIVE ? 0.0 : 1.0);
 }
 
 // Link coefficients of the headloss stage (dgga/solver.py:2923-2956).
@@ -341,6 +350,18 @@ __device__ __forceinline__ void prv_open(const DevNet& n, int i, double qk, int 
 __device__ __forceinline__ void link_coef(const DevNet& n, const PumpTh& th, int k, double q,
                                           int s, double r, bool adj, double& P, double& Y) {
   const int kd = n.kind[k];
+  if (kd == WDS_KIND_FCV) {  // the valve pass fills the GGA coefficients
+    if (!adj) {
+      P = 0.0;
+      Y = 0.0;
+    } else if (s == WDS_ACTIVE) {  // hloss = CBIG (q - qset), hgrad = CBIG
+      P = 1.0 / kCBIG;
+      Y = q - n.fcv_qs[n.link_fcv[k]];
+    } else {
+      valve_state_coef(n, n.fcv_km[n.link_fcv[k]], q, s, P, Y);
+    }
+    return;
+  }
   if (kd == WDS_KIND_PRV) {
     if (!adj) {
       P = 0.0;
@@ -878,7 +899,36 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
   for (int t = tid; t < n.nfill; t += NT) wp<FT>(s)[T.fill[t]] = FT(0);
   gsync<NT>();
   if (tid == 0) {  // valvecoeffs after nodecoeffs, in valve order
-    for (int i = 0; i < n.npcv; ++i) {
+    for (int v = 0; v < n.npcv + n.nfcv; ++v) {
+      const int o = n.vord[v];
+      if (o < 0) {  // FCV (fcvcoeff, hydcoeffs.c:1047-1097 as in dgga/solver.py:1665-1695)
+        const int f = -1 - o, k = n.fcv_link[f];
+        const double qk = s.q[k];
+        const int j1 = n.fcv_j1[f], j2 = n.fcv_j2[f];
+        FT* W = wp<FT>(s);
+        double pk, yk;
+        if (s.S[k] == WDS_ACTIVE) {
+          // the setting cuts the network: an outflow at n1, an inflow at n2
+          const double qs = n.fcv_qs[f];
+          if (n.fcv_xf1[f] >= 0) s.xf[n.fcv_xf1[f]] -= qs;
+          if (n.fcv_xf2[f] >= 0) s.xf[n.fcv_xf2[f]] += qs;
+          yk = qk - qs;
+          s.V0[j1] -= qs;
+          s.V0[j2] += qs;
+          pk = 1.0 / kCBIG;
+        } else {
+          valve_state_coef(n, n.fcv_km[f], qk, s.S[k], pk, yk);
+          s.V0[j1] += yk - qk;
+          s.V0[j2] -= yk - qk;
+        }
+        W[n.fcv_off[f]] += (FT)(-pk);
+        W[T.colptr[j1]] += (FT)pk;
+        W[T.colptr[j2]] += (FT)pk;
+        s.P[k] = pk;
+        s.Y[k] = yk;
+        continue;
+      }
+      const int i = o;
       const int k = n.pcv_link[i];
       const double qk = s.q[k];
       const int sk = s.S[k];
@@ -1305,6 +1355,15 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
           }
         } else if ((n.flags[k] & WDS_F_PUMP_LIVE) && st >= WDS_OPEN) {  // pumpstatus
           st = (-dh > n.phmax[k] + n.htol) ? WDS_XHEAD : WDS_OPEN;
+        }
+        if (n.kind[k] == WDS_KIND_FCV) {
+          // fcvstatus (hydstatus.c:362-398 as in dgga/solver.py:1816-1826,
+          // 1875-1877), from the status before the reopening
+          st = st0;
+          if (dh < -n.htol || qk < -n.qtol)
+            st = WDS_XFCV;
+          else if (st0 == WDS_XFCV && qk >= n.fcv_qs[n.link_fcv[k]])
+            st = WDS_ACTIVE;
         }
         const int t = n.link_tl[k];
         if (t >= 0) {  // tankstatus

@@ -123,7 +123,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     if (a < 0 || a >= N || b < 0 || b >= N)
       return fail(WDS_E_ARG, "wds_plan: link end out of range");
     int kd = net->link_kind[k];
-    if (kd < WDS_KIND_PIPE || kd > WDS_KIND_PRV)
+    if (kd < WDS_KIND_PIPE || kd > WDS_KIND_FCV)
       return fail(WDS_E_UNSUPPORTED, "wds_plan: unsupported link kind");
   }
   // ---- junction graph
@@ -380,6 +380,26 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     pcv_km.push_back(net->km[k]);
   }
   const int npcv = (int)pcv_link.size();
+  // ---- status-machine FCVs, and the valve pass order (link order)
+  std::vector<int> link_fcv(L, -1), fcv_link, fcv_j1, fcv_j2, fcv_off, fcv_xf1, fcv_xf2, vord;
+  std::vector<double> fcv_qs, fcv_km;
+  for (int k = 0; k < L; ++k) {
+    if (net->link_kind[k] == WDS_KIND_PRV) vord.push_back(link_pcv[k]);
+    if (net->link_kind[k] != WDS_KIND_FCV) continue;
+    if (e1[k] < 0 || e2[k] < 0)
+      return fail(WDS_E_UNSUPPORTED, "wds_plan: an FCV with a setting must join two junctions");
+    link_fcv[k] = (int)fcv_link.size();
+    vord.push_back(-1 - (int)fcv_link.size());
+    fcv_link.push_back(k);
+    fcv_j1.push_back(e1[k]);
+    fcv_j2.push_back(e2[k]);
+    fcv_off.push_back(pair_slot_of[{std::max(e1[k], e2[k]), std::min(e1[k], e2[k])}]);
+    fcv_xf1.push_back(node_xf[e1[k]]);
+    fcv_xf2.push_back(node_xf[e2[k]]);
+    fcv_qs.push_back(net->prv_hset[k]);
+    fcv_km.push_back(net->km[k]);
+  }
+  const int nfcv = (int)fcv_link.size();
   std::vector<int> cb_ptr(Nj + 1, 0), cb_idx;
   {
     std::vector<std::vector<int>> cb(Nj);
@@ -464,6 +484,12 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int i = 0; i < npcv; ++i)
       ok = ok && in(pcv_j1[i], 0, Nj) && in(pcv_j2[i], 0, Nj) && in(pcv_off[i], 0, nnzL) &&
            in(pcv_xf[i], 0, std::max(nxf, 1)) && in(pcv_link[i], 0, L);
+    for (int f = 0; f < nfcv; ++f)
+      ok = ok && in(fcv_j1[f], 0, Nj) && in(fcv_j2[f], 0, Nj) && in(fcv_off[f], 0, nnzL) &&
+           in(fcv_xf1[f], -1, std::max(nxf, 1)) && in(fcv_xf2[f], -1, std::max(nxf, 1)) &&
+           in(fcv_link[f], 0, L);
+    ok = ok && (int)vord.size() == npcv + nfcv;
+    for (int v : vord) ok = ok && (v >= 0 ? v < npcv : (-1 - v) < nfcv);
     for (int p = 0; p < Nj; ++p) ok = ok && node_xf[p] < std::max(nxf, 1);
     for (int t = 0; t < ntl; ++t) ok = ok && in(tl_tank[t], 0, Nf) && endok(tl_other[t]);
     for (int k = 0; k < L; ++k) {
@@ -505,7 +531,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       const int k = inc[e];
       const int other = e < inc_split[p] ? e2[k] : e1[k];
       uint32_t v = (uint32_t)k;
-      if (net->link_kind[k] == WDS_KIND_PRV) v |= 1u << 16;
+      if (net->link_kind[k] == WDS_KIND_PRV || net->link_kind[k] == WDS_KIND_FCV) v |= 1u << 16;
       if (other < 0) v |= (1u << 17) | ((uint32_t)(-other - 1) << 18);
       s_in[e] = v;
     }
@@ -514,7 +540,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   std::vector<uint16_t> s_pp(pair_ptr.begin(), pair_ptr.end());
   std::vector<uint16_t> s_pl(pair_link.size());
   for (size_t e = 0; e < pair_link.size(); ++e)
-    s_pl[e] = (uint16_t)(pair_link[e] | (net->link_kind[pair_link[e]] == WDS_KIND_PRV ? 0x8000 : 0));
+    s_pl[e] = (uint16_t)(pair_link[e] | ((net->link_kind[pair_link[e]] == WDS_KIND_PRV ||
+                                          net->link_kind[pair_link[e]] == WDS_KIND_FCV) ? 0x8000 : 0));
   if (s_pl.empty()) s_pl.push_back(0);
   struct TabOff { int sp, fp, cp, ri, lp, rp, re, md, ip, is, in, e1, e2, pp, pl, ps, fl, ds; };
   auto pack = [&](auto tag, Blob& sb, TabOff& o) {
@@ -606,7 +633,10 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
          o_pkm = blob.add(pcv_km), o_tll = blob.add(tl_link), o_tlt = blob.add(tl_tank),
          o_tlo = blob.add(tl_other), o_tlq = blob.add(tl_qsign), o_tlx = blob.add(tl_hmax),
          o_tln = blob.add(tl_hmin), o_tlf = blob.add(tl_flags), o_stab = blob.add(stab_bytes),
-         o_lpu = blob.add(link_pump), o_phu = blob.add(phu);
+         o_lpu = blob.add(link_pump), o_phu = blob.add(phu), o_lfc = blob.add(link_fcv),
+         o_fcl = blob.add(fcv_link), o_fj1 = blob.add(fcv_j1), o_fj2 = blob.add(fcv_j2),
+         o_fof = blob.add(fcv_off), o_fx1 = blob.add(fcv_xf1), o_fx2 = blob.add(fcv_xf2),
+         o_fqs = blob.add(fcv_qs), o_fkm = blob.add(fcv_km), o_vord = blob.add(vord);
   WdsPlan* plan = new WdsPlan();
   if (cudaMalloc(&plan->dtab, blob.bytes.size()) != cudaSuccess) {
     delete plan;
@@ -630,6 +660,10 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.ph0 = P_(double, o_ph0); d.pr = P_(double, o_pr); d.pn = P_(double, o_pn);
   d.pspeed = P_(double, o_psp); d.phmax = P_(double, o_phm); d.cptr = P_(int, o_cptr);
   d.phunit = P_(double, o_phu); d.link_pump = P_(int, o_lpu); d.npump = npump;
+  d.nfcv = nfcv; d.link_fcv = P_(int, o_lfc); d.fcv_link = P_(int, o_fcl);
+  d.fcv_j1 = P_(int, o_fj1); d.fcv_j2 = P_(int, o_fj2); d.fcv_off = P_(int, o_fof);
+  d.fcv_xf1 = P_(int, o_fx1); d.fcv_xf2 = P_(int, o_fx2); d.fcv_qs = P_(double, o_fqs);
+  d.fcv_km = P_(double, o_fkm); d.vord = P_(int, o_vord);
   d.cx = P_(double, o_cx); d.cy = P_(double, o_cy); d.link_tl = P_(int, o_ltl);
   d.link_pcv = P_(int, o_lpcv); d.jnode = P_(int, o_jn); d.el = P_(double, o_el);
   d.inc_ptr = P_(int, o_incp); d.inc_split = P_(int, o_incs); d.inc = P_(int, o_inc);

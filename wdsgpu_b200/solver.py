@@ -194,7 +194,7 @@ class GGASolver:
         self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
         lt = np.asarray(net.link_type, dtype=np.int64)
         nt = np.asarray(net.node_type, dtype=np.int64)
-        allowed = ({CVPIPE, PIPE, TCV, PUMP, PRV} if self.dense_status_machine
+        allowed = ({CVPIPE, PIPE, TCV, PUMP, PRV, FCV} if self.dense_status_machine
                    else {PIPE, TCV, PUMP})
         bad = set(lt.tolist()) - allowed
         if bad:
@@ -314,6 +314,13 @@ class GGASolver:
         pcv = prv & (K0 != MISSING)
         kind[prv & ~pcv] = _lib.KIND_PRV_FIXED
         kind[pcv] = _lib.KIND_PRV
+        # FCVs with a flow setting take the valve pass and fcvstatus; a fixed
+        # (MISSING setting) FCV is a fixed open/closed valve like a fixed PRV
+        fcv = lt == FCV
+        fcvs = fcv & (K0 != MISSING)
+        kind[fcv & ~fcvs] = _lib.KIND_PRV_FIXED
+        kind[fcvs] = _lib.KIND_FCV
+        self.fcv_links = np.flatnonzero(fcvs)
         self.has_cv = bool((lt == CVPIPE).any())
         self.n_pcv = int(pcv.sum())
         self.pcv_links = np.flatnonzero(pcv)
@@ -330,9 +337,17 @@ class GGASolver:
                 raise NotImplementedError(
                     "mode=dense batched PRVs need junctions at both ends: %s"
                     % [net.link_id[int(k)] for k in badp])
+        if self.fcv_links.size:
+            badf = self.fcv_links[is_fixed[n1[self.fcv_links]] | is_fixed[n2[self.fcv_links]]]
+            if badf.size:
+                raise NotImplementedError(
+                    "mode=dense batched FCVs need junctions at both ends: %s"
+                    % [net.link_id[int(k)] for k in badf])
         elev = np.asarray(net.elev_ft, dtype=np.float64)
+        # valve settings: PRV head El[n2] + setting (ft), FCV flow setting (cfs)
         prv_hset = np.zeros(L)
         prv_hset[pcv] = elev[n2[pcv]] + K0[pcv]
+        prv_hset[fcvs] = K0[fcvs]
         # initial flows (hydraul.c initlinkflow as restated in solver.py:2163-2174)
         q = PI * diam ** 2 / 4.0
         if pl.size:

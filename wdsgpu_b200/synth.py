@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .net import (JUNCTION, RESERVOIR, TANK, PIPE, PRV, PUMP, TCV,
+from .net import (JUNCTION, RESERVOIR, TANK, PIPE, PRV, PUMP, TCV, FCV,
                   LPSperCFS, MperFT, Net)
 
 _M3S_PER_CFS = LPSperCFS / 1000.0        # 0.028317 m3/s per cfs
@@ -550,6 +550,31 @@ def chp_dead_end_network(demand_cfs=2e-4, seed=5):
     f["dem_node"] = np.append(net.dem_node, x).astype(np.int32)
     f["dem_base_cfs"] = np.append(net.dem_base_cfs, demand_cfs)
     f["dem_pat"] = np.append(net.dem_pat, -1).astype(np.int32)
+    return Net(**f)
+
+
+def fcv_network(seed=5, links=(62, 22), settings_lps=(14.0, 70.0), km=0.5):
+    """The feature network (PRVs, pumps, tank, emitters) with two junction-to-
+    junction pipes turned into flow control valves with a setting: the first
+    below its pipe's natural flow (an ACTIVE throttle), the second far above
+    it (the network cannot push that much, so fcvstatus takes it to XFCV, an
+    open valve).  Link orientation follows the natural flow."""
+    net = feature_network(seed=seed)
+    f = net.as_fields()
+    lt = np.asarray(net.link_type).copy()
+    st = np.asarray(net.init_status).copy()
+    vs = np.asarray(net.valve_setting_user, dtype=np.float64).copy()
+    kmi = np.asarray(net.km_int, dtype=np.float64).copy()
+    d = np.asarray(net.diam_ft, dtype=np.float64)
+    for k, q in zip(links, settings_lps):
+        lt[k] = FCV
+        st[k] = 2
+        vs[k] = q
+        kmi[k] = 0.02517 * km / (d[k] ** 2 * d[k] ** 2)
+    f["link_type"] = lt.astype(np.int8)
+    f["init_status"] = st.astype(np.int8)
+    f["valve_setting_user"] = vs
+    f["km_int"] = kmi
     return Net(**f)
 
 
