@@ -36,7 +36,8 @@ enum {
   WDS_KIND_PUMP = 3,      /* pump (curve kind in pump_type)          */
   WDS_KIND_PRV_FIXED = 4, /* PRV with MISSING setting: fixed open/closed valve */
   WDS_KIND_PRV = 5,       /* PRV with a setting: status-machine valve */
-  WDS_KIND_FCV = 6        /* FCV with a flow setting: valve pass + fcvstatus (both ends junctions) */
+  WDS_KIND_FCV = 6,       /* FCV with a flow setting: valve pass + fcvstatus (both ends junctions) */
+  WDS_KIND_PSV = 7        /* PSV with a setting: status-machine valve holding H[n1] (both ends junctions) */
 };
 
 /* status codes (EPANET StatusType, dgga/solver.py:1279-1281) */
@@ -99,7 +100,8 @@ typedef struct WdsNetwork {
   const double* curve_x;         /* custom-curve flows (user units)         */
   const double* curve_y;         /* custom-curve heads (user units)         */
   const double* prv_hset;        /* [L] valve setting: El[n2] + setting (ft) for WDS_KIND_PRV,
-                                    the flow setting (cfs) for WDS_KIND_FCV      */
+                                    El[n1] + setting (ft) for WDS_KIND_PSV, the flow
+                                    setting (cfs) for WDS_KIND_FCV               */
   int32_t n_tank_links;
   const int32_t* tl_link;        /* [T] link index                          */
   const int32_t* tl_tank;        /* [T] tank node                           */

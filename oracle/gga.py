@@ -205,16 +205,24 @@ class Model:
         self.tl_is_pump = self.is_pump[k]
         self.tl_pump_in = self.is_pump[k] & (n2[k] == tank)
         self.tl_pump_out = self.is_pump[k] & (n1[k] == tank)
-        # PRVs (solver.py:745-832)
-        prv = np.flatnonzero(lt == _PRV)
+        # PRVs (solver.py:745-832) and PSVs (psvcoeff / psvstatus of the EPANET
+        # replica, solver.py:1647-1664, 1736-1765), with a setting, link order
+        prv = np.flatnonzero((lt == _PRV) | (lt == _PSV))
         self.pcv = prv[K0[prv] != MISSING]
         self.prv_fixed = np.zeros(L, dtype=bool)
         self.prv_fixed[prv[K0[prv] == MISSING]] = True
         self.pcv_mask = np.zeros(L, dtype=bool)
         self.pcv_mask[self.pcv] = True
+        self.prv_psv = lt[self.pcv] == _PSV
         self.prv_n1, self.prv_n2 = n1[self.pcv], n2[self.pcv]
         self.prv_j1, self.prv_j2 = jrow[self.prv_n1], jrow[self.prv_n2]
-        self.prv_hset = self.el[self.prv_n2] + K0[self.pcv]
+        # the head an ACTIVE valve holds (PRV n2, PSV n1), its other end, and
+        # the sign of the valve flow at the held node
+        self.prv_nc = np.where(self.prv_psv, self.prv_n1, self.prv_n2)
+        self.prv_jc = np.where(self.prv_psv, self.prv_j1, self.prv_j2)
+        self.prv_jo = np.where(self.prv_psv, self.prv_j2, self.prv_j1)
+        self.prv_sgn = np.where(self.prv_psv, -1.0, 1.0)
+        self.prv_hset = self.el[self.prv_nc] + K0[self.pcv]
         self.prv_km = self.km[self.pcv]
         # FCVs with a flow setting (fcvcoeff / fcvstatus of the EPANET replica,
         # solver.py:1665-1695, 1816-1826, 1875-1877); fixed ones are fixed valves
@@ -473,19 +481,20 @@ class Model:
                 po, yo = np.full_like(qk, 1.0 / CSMALL), qk
             pna = np.where(cl, 1.0 / CBIG, po) * (~act)
             yna = np.where(cl, qk, yo)
-            xf2 = Xflow[:, j2]
+            jc, jo, sg = self.prv_jc[i], self.prv_jo[i], self.prv_sgn[i]
+            xfc = Xflow[:, jc]
             dy = (yna - qk) * (~act)
-            f1 = dy + np.where(act & (xf2 < 0.0), xf2, 0.0)
-            f2 = -dy + self.prv_hset[i] * CBIG * act
             if A is not None:
                 for slot, v in ((j1 * Nj + j2, -pna), (j2 * Nj + j1, -pna),
                                 (j1 * Nj + j1, pna), (j2 * Nj + j2, pna),
-                                (j2 * Nj + j2, CBIG * act)):
+                                (jc * Nj + jc, CBIG * act)):
                     A[:, slot] += v
-            F[:, j1] += f1
-            F[:, j2] += f2
+            F[:, j1] += dy
+            F[:, j2] -= dy
+            F[:, jo] += np.where(act & (sg * xfc < 0.0), xfc, 0.0)
+            F[:, jc] += self.prv_hset[i] * CBIG * act
             P[:, k] = pna
-            Y[:, k] = np.where(act, qk + xf2, yna)
+            Y[:, k] = np.where(act, qk + sg * xfc, yna)
         return P, Y, F, A
 
     # ---------------------------------------------------------- status
@@ -542,6 +551,15 @@ class Model:
         c_cl = np.where((h1 >= hs + ht) & (h2 < hs - ht), ACTIVE,
                         np.where((h1 < hs - ht) & (h1 > h2 + ht), OPEN, CLOSED))
         c_xp = np.where(neg, CLOSED, sk)
+        if self.prv_psv.any():   # psvstatus (solver.py:1736-1765)
+            v = self.prv_psv
+            c_act = np.where(v, np.where(neg, CLOSED, np.where(h2 + hml > hs + ht, OPEN, ACTIVE)),
+                             c_act)
+            c_open = np.where(v, np.where(neg, CLOSED, np.where(h1 < hs - ht, ACTIVE, OPEN)),
+                              c_open)
+            c_cl = np.where(v, np.where((h2 > hs + ht) & (h1 > h2 + ht), OPEN,
+                                        np.where((h1 >= hs + ht) & (h1 > h2 + ht), ACTIVE, CLOSED)),
+                            c_cl)
         new = np.where(sk == ACTIVE, c_act, np.where(sk == OPEN, c_open,
                        np.where(sk == CLOSED, c_cl, np.where(sk == XPRESSURE, c_xp, sk))))
         new = new.astype(np.int8)
@@ -726,7 +744,7 @@ class Model:
         out = out + emh * x
         if act is not None:
             for b in range(x.shape[0]):
-                np.add.at(out[b], self.prv_j2, x[b, self.prv_j2] * act[b] * CBIG)
+                np.add.at(out[b], self.prv_jc, x[b, self.prv_jc] * act[b] * CBIG)
         return out
 
     def factor(self, P, emh, act, lu=False):
@@ -741,7 +759,7 @@ class Model:
         A[:, diag] += emh
         if act is not None and act.any():
             for b in range(B):
-                np.add.at(A[b], self.prv_j2 * (Nj + 1), CBIG * act[b])
+                np.add.at(A[b], self.prv_jc * (Nj + 1), CBIG * act[b])
         A = A.reshape(B, Nj, Nj)
         if lu:
             return [("lu", sla.lu_factor(A[b])) for b in range(B)]
@@ -763,7 +781,7 @@ class Model:
         if act is None or not act.any():
             return self._solveA(kf, P, emh, act, rhs)
         B, p = rhs.shape[0], act.shape[1]
-        j1, j2 = self.prv_j1, self.prv_j2
+        j1, j2 = self.prv_jo, self.prv_jc     # other end, held node
         actf = act.astype(float)
         rp = rhs.copy()
         for b in range(B):
@@ -805,7 +823,7 @@ class Model:
         r_l = hl - (H[:, self.n1] - H[:, self.n2])
         r_prv = None
         if act is not None:
-            r_prv = (H[:, self.prv_n2] - self.prv_hset) * act
+            r_prv = (H[:, self.prv_nc] - self.prv_hset) * act
         hle, _ = self.emitter(e, ke)
         r_e = hle - (H[:, self.junc] - self.el_j)
         m = _scatter(self.Nj, self.f2, q[:, self.lk_m2])
@@ -830,8 +848,8 @@ class Model:
             dq = -P * (r_l + (dH[:, self.j2c] * self.m2f - dH[:, self.j1c] * self.m1f))
             if act is not None and act.any():
                 base = self.matvec(P, emh, act, dH)
-                ab2 = base[:, self.prv_j2] - CBIG * dH[:, self.prv_j2] * act
-                dqp = rhs[:, self.prv_j2] - ab2
+                ab2 = base[:, self.prv_jc] - CBIG * dH[:, self.prv_jc] * act
+                dqp = self.prv_sgn * (rhs[:, self.prv_jc] - ab2)
                 dq[:, self.pcv] = np.where(act, dqp, dq[:, self.pcv])
             de = em * (-r_e + dH) / hge
             q = q + dq
@@ -846,10 +864,10 @@ class Model:
         if act is None or not act.any():
             return self._solveA(kf, P, emh, act, r)
         B, p = r.shape[0], act.shape[1]
-        j1, j2 = self.prv_j1, self.prv_j2
+        j1, j2 = self.prv_jo, self.prv_jc     # other end, held node
         actf = act.astype(float)
         r2 = r.copy()
-        r2[:, j2] = np.where(act, gQp, r[:, j2])
+        r2[:, j2] = np.where(act, self.prv_sgn * gQp, r[:, j2])
         x0 = self._solveA(kf, P, emh, act, r2)
         cols = []
         for u in j2:

@@ -21,6 +21,7 @@ Usage:  python tests/golden/make_golden.py        (steady cases)
         python tests/golden/make_golden.py pumps  (pump-parameter gradient pins, pump_ref.npz
                                                    and chp_ref.npz)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
+        python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
 """
 import json
 import os
@@ -343,25 +344,15 @@ def make_pumps():
                [1, 1, 1, 1.05], "chp_ref")
 
 
-def make_fcv():
-    """FCV pin: the reference's EPANET replica (mode="epanet",
-    status_machine=True, dgga/solver.py:1922-2130: fcvcoeff, fcvstatus in
-    linkstatus, valve-order Xflow) on the feature network with two FCVs, one
-    throttling (ACTIVE) and one pushed beyond what the network delivers
-    (XFCV), four scenarios; then the reference's CPU implicit adjoint
-    (ImplicitGGASolve, dgga/autodiff.py:609-756) with each scenario's final
-    statuses frozen, for L = sum of squared sensor heads + squared FCV flows."""
-    import torch
-    sys.path.insert(0, REPO)
+def _valve_case(dgga, torch, net, d, rh, links, name):
+    """The reference's EPANET replica (mode="epanet", status_machine=True,
+    dgga/solver.py:1922-2130) per scenario, then its CPU implicit adjoint
+    (ImplicitGGASolve, dgga/autodiff.py:609-756) with that scenario's final
+    statuses frozen, for L = sum of squared sensor heads + squared flows of
+    the given valve links."""
     from wdsgpu_b200 import synth
-    dgga = _load_reference()
-    torch.set_default_dtype(torch.float64)
-    net = synth.fcv_network()
-    d, _ = synth.config2_scenarios(net, 4, seed=23, sigma=0.3)
-    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
     ke = np.asarray(net.node_ke, dtype=np.float64)
     sens = synth.sensor_nodes(net, 6)
-    fl = np.flatnonzero(np.asarray(net.link_type) == 6)
     ref_net = dgga.parse.Net(**net.as_fields())
     se = dgga.solver.GGASolver(ref_net, device="cpu", mode="epanet")
     keys = ("fwd_head", "fwd_flow", "fwd_status", "fwd_iters", "head", "flow", "g_demand",
@@ -377,19 +368,53 @@ def make_fcv():
         R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
         h, q, e = dgga.autodiff.implicit_solve(se, D, RH, ke=KE, r_hw=R, accuracy=1e-10,
                                                adjoint="cpu", status=st)
-        loss = (h[:, sens] ** 2).sum() + (q[:, fl] ** 2).sum()
+        loss = (h[:, sens] ** 2).sum() + (q[:, links] ** 2).sum()
         loss.backward()
         for k, v in zip(keys, (f["head_ft"], f["flow_cfs"], st, f["iters"], h.detach(),
                                q.detach(), D.grad, KE.grad, R.grad, RH.grad)):
             res[k].append(np.asarray(v).reshape(-1))
     blob = pack_net(net)
-    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens)})
+    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
+                 "in_loss_links": np.asarray(links)})
     blob.update({"ref_" + k: np.stack(v) for k, v in res.items()})
-    path = os.path.join(HERE, "fcv_ref.npz")
+    path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **blob)
-    print("fcv: iters %s, FCV statuses %s -> %s" % (
-        np.stack(res["fwd_iters"]).ravel().tolist(), np.stack(res["fwd_status"])[:, fl].tolist(),
-        os.path.basename(path)))
+    print("%s: iters %s, valve statuses %s -> %s" % (
+        name, np.stack(res["fwd_iters"]).ravel().tolist(),
+        np.stack(res["fwd_status"])[:, links].tolist(), os.path.basename(path)))
+
+
+def make_fcv():
+    """FCV pin: the feature network with two FCVs, one throttling (ACTIVE) and
+    one pushed beyond what the network delivers (XFCV), four scenarios
+    (fcvcoeff, fcvstatus in linkstatus, valve-order Xflow of the replica)."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.fcv_network()
+    d, _ = synth.config2_scenarios(net, 4, seed=23, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    _valve_case(dgga, torch, net, d, rh, np.flatnonzero(np.asarray(net.link_type) == 6),
+                "fcv_ref")
+
+
+def make_psv():
+    """PSV pin: the feature network (ACTIVE PRV) plus a PSV that throttles to
+    hold its upstream pressure, four scenarios (psvcoeff, psvstatus in
+    valvestatus); the loss takes both valves' flows, so the adjoint's
+    constraint rows of both orientations carry a right-hand side."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.psv_network()
+    d, _ = synth.config2_scenarios(net, 4, seed=29, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    lt = np.asarray(net.link_type)
+    _valve_case(dgga, torch, net, d, rh, np.flatnonzero((lt == 3) | (lt == 4)), "psv_ref")
 
 
 if __name__ == "__main__":
@@ -401,5 +426,7 @@ if __name__ == "__main__":
         make_pumps()
     elif sys.argv[1:] == ["fcv"]:
         make_fcv()
+    elif sys.argv[1:] == ["psv"]:
+        make_psv()
     else:
         main()

@@ -1,6 +1,8 @@
-"""Flow control valves on the B200 route (WDS_KIND_FCV): the batched GGA with
-FCVs in the valve pass and fcvstatus, against the reference's EPANET replica
-with its status machine (fixture tests/golden/fcv_ref.npz), its CPU implicit
+"""Flow control and pressure sustaining valves on the B200 route
+(WDS_KIND_FCV, WDS_KIND_PSV): the batched GGA with FCVs in the valve pass and
+fcvstatus, PSVs in the valve pass, psvstatus and the constraint rows at their
+upstream junction, against the reference's EPANET replica with its status
+machine (fixtures tests/golden/fcv_ref.npz, psv_ref.npz), its CPU implicit
 adjoint, and the oracle on unseen scenarios."""
 import os
 import sys
@@ -19,9 +21,10 @@ from oracle.gga import Model  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def test_fcv_forward_matches_reference(cuda):
+@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref"])
+def test_valve_forward_matches_reference(cuda, case):
     from wdsgpu_b200.solver import GGASolver
-    net, inp, ref = load("fcv_ref")
+    net, inp, ref = load(case)
     s = GGASolver(net, device=cuda, dense_status_machine=True)
     out = s.solve(torch.tensor(inp["demand"], device=cuda),
                   torch.tensor(inp["res_head"], device=cuda),
@@ -31,10 +34,11 @@ def test_fcv_forward_matches_reference(cuda):
     assert np.abs(out["head_ft"].cpu().numpy() - ref["fwd_head"]).max() < 1e-4
 
 
-def test_fcv_gradients_match_reference(cuda):
+@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref"])
+def test_valve_gradients_match_reference(cuda, case):
     from wdsgpu_b200.autodiff import implicit_solve
     from wdsgpu_b200.solver import GGASolver
-    net, inp, ref = load("fcv_ref")
+    net, inp, ref = load(case)
     s = GGASolver(net, device=cuda, dense_status_machine=True)
     B = inp["demand"].shape[0]
     D = torch.tensor(inp["demand"], device=cuda).requires_grad_(True)
@@ -42,7 +46,7 @@ def test_fcv_gradients_match_reference(cuda):
     KE = torch.tensor(np.tile(inp["ke"], (B, 1)), device=cuda).requires_grad_(True)
     R = torch.tensor(np.tile(np.asarray(net.r_hw), (B, 1)), device=cuda).requires_grad_(True)
     h, q, e = implicit_solve(s, D, RH, ke=KE, r_hw=R, accuracy=1e-7)
-    fl = torch.as_tensor(np.flatnonzero(np.asarray(net.link_type) == 6), device=cuda)
+    fl = torch.as_tensor(np.asarray(inp["loss_links"]), device=cuda)
     sens = torch.as_tensor(np.asarray(inp["sensors"]), device=cuda)
     ((h[:, sens] ** 2).sum() + (q[:, fl] ** 2).sum()).backward()
     assert np.abs(h.detach().cpu().numpy() - ref["head"]).max() < 1e-9
@@ -54,11 +58,12 @@ def test_fcv_gradients_match_reference(cuda):
         assert np.abs(gi - Rf).max() <= 1e-8 * np.abs(Rf).max(), (key, np.abs(gi - Rf).max())
 
 
-def test_fcv_unseen_scenarios_against_oracle(cuda):
+@pytest.mark.parametrize("which", ["fcv", "psv"])
+def test_valve_unseen_scenarios_against_oracle(cuda, which):
     from wdsgpu_b200 import synth
     from wdsgpu_b200.autodiff import implicit_solve
     from wdsgpu_b200.solver import GGASolver
-    net = synth.fcv_network()
+    net = synth.fcv_network() if which == "fcv" else synth.psv_network()
     d, _ = synth.config2_scenarios(net, 12, seed=97, sigma=0.4)
     rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
     s = GGASolver(net, device=cuda, dense_status_machine=True)

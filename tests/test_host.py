@@ -19,9 +19,10 @@ def test_unsupported_link_types_raise():
         GGASolver(net, device="cpu", dense_status_machine=False)
     n2 = copy.deepcopy(net)
     n2.link_type = n2.link_type.copy()
-    n2.link_type[0] = PSV
+    n2.link_type[0] = PSV                          # batched PSVs (status machine only)
+    GGASolver(n2, device="cpu", dense_status_machine=True)
     with pytest.raises(NotImplementedError):
-        GGASolver(n2, device="cpu", dense_status_machine=True)
+        GGASolver(n2, device="cpu", dense_status_machine=False)
     n2.link_type[0] = PBV
     with pytest.raises(NotImplementedError):
         GGASolver(n2, device="cpu", dense_status_machine=True)

@@ -1,8 +1,10 @@
-"""Flow control valve pin: the oracle's batched FCV (valve-order fcvcoeff,
-fcvstatus at the link-status checks) against the reference's EPANET replica
-with its status machine (fixture tests/golden/fcv_ref.npz, `make_golden.py
-fcv`): iteration counts and statuses exact, heads, and the CPU implicit
-adjoint's gradients with the final statuses frozen."""
+"""Flow control and pressure sustaining valve pins: the oracle's batched FCV
+(valve-order fcvcoeff, fcvstatus at the link-status checks) and PSV
+(psvcoeff, psvstatus, constraint rows at the upstream junction) against the
+reference's EPANET replica with its status machine (fixtures
+tests/golden/fcv_ref.npz and psv_ref.npz, `make_golden.py fcv` / `psv`):
+iteration counts and statuses exact, heads, and the CPU implicit adjoint's
+gradients with the final statuses frozen."""
 import os
 import sys
 
@@ -16,12 +18,13 @@ from golden.load import load  # noqa: E402
 from oracle.gga import Model  # noqa: E402
 
 
-def fcv_loss_grads(m, net, inp, accuracy=1e-7):
-    """Oracle implicit solve and the adjoint of L = sum h[sensors]^2 + sum q[FCVs]^2."""
+def valve_loss_grads(m, net, inp, accuracy=1e-7):
+    """Oracle implicit solve and the adjoint of L = sum h[sensors]^2 +
+    sum q[loss links]^2 (the valve links the fixture names)."""
     d, rh = inp["demand"], inp["res_head"]
     out, st = m.implicit(d, rh, ke=inp["ke"], accuracy=accuracy)
     B = d.shape[0]
-    fl = np.flatnonzero(np.asarray(net.link_type) == 6)
+    fl = np.asarray(inp["loss_links"])
     H, q = out["head_ft"], out["flow_cfs"]
     gH = np.zeros((B, net.N))
     for b in range(B):
@@ -46,10 +49,29 @@ def test_oracle_fcv_forward_matches_reference():
 
 def test_oracle_fcv_adjoint_matches_reference():
     net, inp, ref = load("fcv_ref")
-    out, g = fcv_loss_grads(Model(net), net, inp)
+    out, g = valve_loss_grads(Model(net), net, inp)
     assert np.abs(out["head_ft"] - ref["head"]).max() < 1e-9
     fixed = np.asarray(net.node_type) != 0
     for gi, key, cols in ((g[0], "g_demand", slice(None)), (g[2], "g_ke", slice(None)),
                           (g[3], "g_rhw", slice(None)), (g[1], "g_res_head", fixed)):
         R = ref[key][:, cols]           # one reference call per scenario: per-scenario rows
+        assert np.abs(gi[:, cols] - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi[:, cols] - R).max())
+
+
+def test_oracle_psv_matches_reference():
+    """PSV pin (fixture tests/golden/psv_ref.npz): the ACTIVE PSV holds its
+    upstream head; together with the network's ACTIVE PRV the adjoint has
+    constraint rows of both orientations."""
+    net, inp, ref = load("psv_ref")
+    out = Model(net).solve(inp["demand"], inp["res_head"], ke=inp["ke"], accuracy=1e-7,
+                           status_machine=True)
+    np.testing.assert_array_equal(out["iters"], ref["fwd_iters"].ravel())
+    np.testing.assert_array_equal(out["status"], ref["fwd_status"])
+    assert np.abs(out["head_ft"] - ref["fwd_head"]).max() < 1e-4
+    out, g = valve_loss_grads(Model(net), net, inp)
+    assert np.abs(out["head_ft"] - ref["head"]).max() < 1e-9
+    fixed = np.asarray(net.node_type) != 0
+    for gi, key, cols in ((g[0], "g_demand", slice(None)), (g[2], "g_ke", slice(None)),
+                          (g[3], "g_rhw", slice(None)), (g[1], "g_res_head", fixed)):
+        R = ref[key][:, cols]
         assert np.abs(gi[:, cols] - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi[:, cols] - R).max())

@@ -15,7 +15,7 @@ c_int32_p = ctypes.POINTER(ctypes.c_int32)
 c_int64_p = ctypes.POINTER(ctypes.c_int64)
 c_double_p = ctypes.POINTER(ctypes.c_double)
 
-KIND_PIPE, KIND_CVPIPE, KIND_TCV, KIND_PUMP, KIND_PRV_FIXED, KIND_PRV, KIND_FCV = range(7)
+KIND_PIPE, KIND_CVPIPE, KIND_TCV, KIND_PUMP, KIND_PRV_FIXED, KIND_PRV, KIND_FCV, KIND_PSV = range(8)
 F_ZERO_SPEED, F_PUMP_LIVE, F_CHP, F_IS_PIPE = 1, 2, 4, 8
 TL_OVERFLOW, TL_IS_PUMP, TL_PUMP_IN, TL_PUMP_OUT = 1, 2, 4, 8
 INFO_NOT_PD, INFO_UNCONVERGED, INFO_EMITTER_CAP = 1, 2, 4

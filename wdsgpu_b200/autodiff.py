@@ -47,15 +47,15 @@ def _adjoint_guards(s: GGASolver, flow, S, pumps=None, allow_clamp=False):
     entries are returned as (scenario, link, assembled P) tensors (None when
     there are none) for `_clamp_rhs`."""
     if s.n_pcv:
-        j1 = s._n1[s.pcv_links]
-        j2 = s._n2[s.pcv_links]
-        if np.unique(j2).size < j2.size:
+        # the junction each PRV (n2) or PSV (n1) holds, and its other end
+        jc, jo = s.pcv_jc, s.pcv_jo
+        if np.unique(jc).size < jc.size:
             raise NotImplementedError(
-                "adjoint='gpu': several PRVs share one downstream junction")
-        if np.intersect1d(j2, j1).size:
+                "adjoint='gpu': several PRVs/PSVs hold one junction")
+        if np.intersect1d(jc, jo).size:
             raise NotImplementedError(
-                "adjoint='gpu': cascaded PRVs (a downstream junction is another "
-                "PRV's upstream junction)")
+                "adjoint='gpu': cascaded PRVs/PSVs (a held junction is another "
+                "valve's other end)")
     chp = s._tables["pump_type"] == 0
     if not chp.any():
         return None

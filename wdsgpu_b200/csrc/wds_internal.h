@@ -80,9 +80,15 @@ struct DevNet {
   const int* pcv_j1;
   const int* pcv_j2;
   const int* pcv_off;     // slot of (j1,j2)
-  const int* pcv_xf;      // Xflow slot of j2
+  const int* pcv_xf;      // Xflow slot of jc
   const double* pcv_hset;
   const double* pcv_km;
+  // the head an ACTIVE valve holds: PRV at j2 (flow enters it, sgn +1), PSV
+  // at j1 (flow leaves it, sgn -1); jo is the other end
+  const int* pcv_jc;
+  const int* pcv_jo;
+  const double* pcv_sgn;
+  const int* pcv_psv;     // 1 for a PSV (psvstatus), 0 for a PRV
   // status-machine FCVs [nfcv] (valve pass and fcvstatus; never constraint rows)
   int nfcv;
   const int* link_fcv;    // [L] fcv index or -1

@@ -362,7 +362,7 @@ __device__ __forceinline__ void link_coef(const DevNet& n, const PumpTh& th, int
     }
     return;
   }
-  if (kd == WDS_KIND_PRV) {
+  if (kd == WDS_KIND_PRV || kd == WDS_KIND_PSV) {
     if (!adj) {
       P = 0.0;
       Y = 0.0;
@@ -936,20 +936,24 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       double pna, yna;
       prv_open(n, i, qk, sk, pna, yna);
       const double mna = act ? 0.0 : 1.0, mact = act ? 1.0 : 0.0;
-      const double xf2 = s.xf[n.pcv_xf[i]];
+      // prvcoeff / psvcoeff (hydcoeffs.c:959-1044 as in dgga/solver.py:
+      // 862-903, 1647-1664): an ACTIVE valve holds the head of jc (PRV: n2,
+      // PSV: n1) by a CBIG penalty and reads the flow excess there
+      const double xfc = s.xf[n.pcv_xf[i]], sg = n.pcv_sgn[i];
       const double dy = (yna - qk) * mna;
-      const double f1 = dy + ((act && xf2 < 0.0) ? xf2 : 0.0);
-      const double f2 = -dy + n.pcv_hset[i] * kCBIG * mact;
-      const int j1 = n.pcv_j1[i], j2 = n.pcv_j2[i];
+      const int j1 = n.pcv_j1[i], j2 = n.pcv_j2[i], jc = n.pcv_jc[i], jo = n.pcv_jo[i];
+      const double fo = (act && sg * xfc < 0.0) ? xfc : 0.0;
       FT* W = wp<FT>(s);
       W[n.pcv_off[i]] += (FT)(-pna);
       W[T.colptr[j1]] += (FT)pna;
       W[T.colptr[j2]] += (FT)pna;
-      W[T.colptr[j2]] += (FT)(kCBIG * mact);
-      s.V0[j1] += f1;
-      s.V0[j2] += f2;
+      W[T.colptr[jc]] += (FT)(kCBIG * mact);
+      s.V0[j1] += dy;
+      s.V0[j2] -= dy;
+      s.V0[jo] += fo;
+      s.V0[jc] += n.pcv_hset[i] * kCBIG * mact;
       s.P[k] = pna;
-      s.Y[k] = act ? qk + xf2 : yna;
+      s.Y[k] = act ? qk + sg * xfc : yna;
     }
   }
   gsync<NT>();
@@ -1028,11 +1032,11 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
   for (int q = tid; q < n.Nj; q += NT) rp[q] = rhs[q];
   gsync<NT>();
   if (tid == 0) {
-    // rp[j1] += rhs[j2] (ACTIVE), then rp[j2] = -r_prv
+    // rp[jo] += rhs[jc] (ACTIVE), then rp[jc] = -r_prv (jc: the held head)
     for (int i = 0; i < p; ++i)
-      if (actf[i] != 0.0) rp[n.pcv_j1[i]] += rhs[n.pcv_j2[i]];
+      if (actf[i] != 0.0) rp[n.pcv_jo[i]] += rhs[n.pcv_jc[i]];
     for (int i = 0; i < p; ++i)
-      if (actf[i] != 0.0) rp[n.pcv_j2[i]] = -rprv[i];
+      if (actf[i] != 0.0) rp[n.pcv_jc[i]] = -rprv[i];
   }
   gsync<NT>();
   // The outer refinement below (two steps against the true M_p) contracts the
@@ -1047,29 +1051,29 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
       gsync<NT>();
       continue;
     }
-    const int u = c < p ? n.pcv_j2[c] : n.pcv_j1[c - p];
+    const int u = c < p ? n.pcv_jc[c] : n.pcv_jo[c - p];
     solve_refined<NT, FT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
   }
   if (tid == 0) {
     // C = [R2 ; I2 - CBIG R2], rows of inactive valves -> identity
     for (int a = 0; a < p; ++a)
       for (int c = 0; c < m; ++c) {
-        const double r2 = cols[(size_t)c * n.Nj + n.pcv_j2[a]];
+        const double r2 = cols[(size_t)c * n.Nj + n.pcv_jc[a]];
         const double i2 = (c == a || c == a + p) ? 1.0 : 0.0;
         C[a * m + c] = actf[a] != 0.0 ? r2 : (c == a ? 1.0 : 0.0);
         C[(a + p) * m + c] = actf[a] != 0.0 ? i2 - kCBIG * r2 : (c == a + p ? 1.0 : 0.0);
       }
   }
   gsync<NT>();
-  // x <- x - S y,  y = C^{-1} [ (x[j2]-rr[j2]) act ; (rr[j2] - CBIG x[j2]) act ]
+  // x <- x - S y,  y = C^{-1} [ (x[jc]-rr[jc]) act ; (rr[jc] - CBIG x[jc]) act ]
   auto wood = [&](double* x, const double* rr) {
     if (tid == 0) {
       double Cc[64];
       for (int i = 0; i < m * m; ++i) Cc[i] = C[i];
       for (int a = 0; a < p; ++a) {
-        const int j2 = n.pcv_j2[a];
-        y[a] = (x[j2] - rr[j2]) * actf[a];
-        y[a + p] = (rr[j2] - kCBIG * x[j2]) * actf[a];
+        const int jc = n.pcv_jc[a];
+        y[a] = (x[jc] - rr[jc]) * actf[a];
+        y[a + p] = (rr[jc] - kCBIG * x[jc]) * actf[a];
       }
       dense_solve(Cc, y, m);
     }
@@ -1087,15 +1091,15 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
     gsync<NT>();
     if (tid == 0)
       for (int i = 0; i < p; ++i)
-        row1[i] = res[n.pcv_j1[i]] + res[n.pcv_j2[i]] - kCBIG * dH[n.pcv_j2[i]];
+        row1[i] = res[n.pcv_jo[i]] + res[n.pcv_jc[i]] - kCBIG * dH[n.pcv_jc[i]];
     gsync<NT>();
     for (int q = tid; q < n.Nj; q += NT) res[q] = rp[q] - res[q];
     gsync<NT>();
     if (tid == 0) {
       for (int i = 0; i < p; ++i)
-        if (actf[i] != 0.0) res[n.pcv_j1[i]] = rp[n.pcv_j1[i]] - row1[i];
+        if (actf[i] != 0.0) res[n.pcv_jo[i]] = rp[n.pcv_jo[i]] - row1[i];
       for (int i = 0; i < p; ++i)
-        if (actf[i] != 0.0) res[n.pcv_j2[i]] = rp[n.pcv_j2[i]] - dH[n.pcv_j2[i]];
+        if (actf[i] != 0.0) res[n.pcv_jc[i]] = rp[n.pcv_jc[i]] - dH[n.pcv_jc[i]];
     }
     gsync<NT>();
     solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 0);
@@ -1317,7 +1321,17 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
       const double hml = n.pcv_km[i] * (qk * qk);
       const bool neg = qk < -n.qtol;
       int ns = sk;
-      if (sk == WDS_ACTIVE)
+      if (n.pcv_psv[i]) {  // psvstatus (hydstatus.c:302-359 as in dgga/solver.py:1736-1765)
+        if (sk == WDS_ACTIVE)
+          ns = neg ? WDS_CLOSED : (h2 + hml > hs + ht ? WDS_OPEN : WDS_ACTIVE);
+        else if (sk == WDS_OPEN)
+          ns = neg ? WDS_CLOSED : (h1 < hs - ht ? WDS_ACTIVE : WDS_OPEN);
+        else if (sk == WDS_CLOSED)
+          ns = (h2 > hs + ht && h1 > h2 + ht) ? WDS_OPEN
+               : ((h1 >= hs + ht && h1 > h2 + ht) ? WDS_ACTIVE : WDS_CLOSED);
+        else if (sk == WDS_XPRESSURE)
+          ns = neg ? WDS_CLOSED : sk;
+      } else if (sk == WDS_ACTIVE)
         ns = neg ? WDS_CLOSED : (h1 - hml < hs - ht ? WDS_OPEN : WDS_ACTIVE);
       else if (sk == WDS_OPEN)
         ns = neg ? WDS_CLOSED : (h2 >= hs + ht ? WDS_ACTIVE : WDS_OPEN);
@@ -1424,7 +1438,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
       bool any_act = false;
       for (int i = gtid<NT>(); i < n.npcv; i += NT) {
         const bool act = s.S[n.pcv_link[i]] == WDS_ACTIVE;
-        rprv[i] = (Hs[n.pcv_j2[i]] - n.pcv_hset[i]) * (act ? 1.0 : 0.0);
+        rprv[i] = (Hs[n.pcv_jc[i]] - n.pcv_hset[i]) * (act ? 1.0 : 0.0);
         any_act |= act;
       }
       any_act = gsync_or<NT>(any_act);
@@ -1460,10 +1474,10 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
-        if (i >= 0 && s.S[k] == WDS_ACTIVE) {
-          const int j2 = n.pcv_j2[i];
-          const double ab2 = amul_node(n, T, s, j2, s.V1) - kCBIG * s.V1[j2] * 1.0;
-          dq = s.V0[j2] - ab2;
+        if (i >= 0 && s.S[k] == WDS_ACTIVE) {  // the free valve flow, from the balance at jc
+          const int jc = n.pcv_jc[i];
+          const double abc = amul_node(n, T, s, jc, s.V1) - kCBIG * s.V1[jc] * 1.0;
+          dq = n.pcv_sgn[i] * (s.V0[jc] - abc);
         }
         s.q[k] = s.q[k] + dq;
       }
@@ -1639,7 +1653,9 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
     gsync<NT>();
     if (gtid<NT>() == 0)
       for (int i = 0; i < p; ++i)
-        if (actf[i] != 0.0) r2[n.pcv_j2[i]] = gQ[n.pcv_link[i]];
+        // row jc: lam[n2] - lam[n1] = gQ of the free valve flow, i.e.
+        // lam[jc] - lam[jo] = sgn gQ (PRV jc = n2, PSV jc = n1)
+        if (actf[i] != 0.0) r2[n.pcv_jc[i]] = n.pcv_sgn[i] * gQ[n.pcv_link[i]];
     gsync<NT>();
     // unrefined solves: the two outer refinement steps below contract their error
     solve_refined<NT, FT>(n, T, s, r2, -1, lam, t, 0);
@@ -1649,12 +1665,12 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
         gsync<NT>();
         continue;
       }
-      solve_refined<NT, FT>(n, T, s, nullptr, n.pcv_j2[c], cols + (size_t)c * n.Nj, t, 0);
+      solve_refined<NT, FT>(n, T, s, nullptr, n.pcv_jc[c], cols + (size_t)c * n.Nj, t, 0);
     }
     if (gtid<NT>() == 0)
       for (int a0 = 0; a0 < p; ++a0)
         for (int c = 0; c < p; ++c) {
-          const double cw = cols[(size_t)c * n.Nj + n.pcv_j2[a0]] - cols[(size_t)c * n.Nj + n.pcv_j1[a0]];
+          const double cw = cols[(size_t)c * n.Nj + n.pcv_jc[a0]] - cols[(size_t)c * n.Nj + n.pcv_jo[a0]];
           C[a0 * p + c] = cw * actf[a0] * actf[c] + (a0 == c ? 1.0 - actf[a0] : 0.0);
         }
     gsync<NT>();
@@ -1663,7 +1679,7 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
         double Cc[64];
         for (int i = 0; i < p * p; ++i) Cc[i] = C[i];
         for (int a0 = 0; a0 < p; ++a0)
-          y[a0] = (x[n.pcv_j2[a0]] - x[n.pcv_j1[a0]] - rr[n.pcv_j2[a0]]) * actf[a0];
+          y[a0] = (x[n.pcv_jc[a0]] - x[n.pcv_jo[a0]] - rr[n.pcv_jc[a0]]) * actf[a0];
         dense_solve(Cc, y, p);
       }
       gsync<NT>();
@@ -1681,7 +1697,7 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
       if (gtid<NT>() == 0)
         for (int i = 0; i < p; ++i)
           if (actf[i] != 0.0)
-            res[n.pcv_j2[i]] = r2[n.pcv_j2[i]] - (lam[n.pcv_j2[i]] - lam[n.pcv_j1[i]]);
+            res[n.pcv_jc[i]] = r2[n.pcv_jc[i]] - (lam[n.pcv_jc[i]] - lam[n.pcv_jo[i]]);
       gsync<NT>();
       solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 0);
       wood(sx, res);

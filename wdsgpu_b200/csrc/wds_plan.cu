@@ -123,7 +123,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     if (a < 0 || a >= N || b < 0 || b >= N)
       return fail(WDS_E_ARG, "wds_plan: link end out of range");
     int kd = net->link_kind[k];
-    if (kd < WDS_KIND_PIPE || kd > WDS_KIND_FCV)
+    if (kd < WDS_KIND_PIPE || kd > WDS_KIND_PSV)
       return fail(WDS_E_UNSUPPORTED, "wds_plan: unsupported link kind");
   }
   // ---- junction graph
@@ -362,20 +362,29 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int e = colptr[j] + 1; e < colptr[j + 1]; ++e)
       if (!is_a[e]) fill_slot.push_back(e);
   // ---- status-machine PRVs
+  // (PRVs and PSVs with a setting, in link order)
   std::vector<int> link_pcv(L, -1), pcv_link, pcv_j1, pcv_j2, pcv_off, pcv_xf, node_xf(Nj, -1);
-  std::vector<double> pcv_hset, pcv_km;
+  std::vector<int> pcv_jc, pcv_jo, pcv_psv;
+  std::vector<double> pcv_hset, pcv_km, pcv_sgn;
   int nxf = 0;
   for (int k = 0; k < L; ++k) {
-    if (net->link_kind[k] != WDS_KIND_PRV) continue;
+    const bool psv = net->link_kind[k] == WDS_KIND_PSV;
+    if (net->link_kind[k] != WDS_KIND_PRV && !psv) continue;
     if (e1[k] < 0 || e2[k] < 0)
-      return fail(WDS_E_UNSUPPORTED, "wds_plan: a PRV with a setting must join two junctions");
+      return fail(WDS_E_UNSUPPORTED,
+                  "wds_plan: a PRV or PSV with a setting must join two junctions");
+    const int jc = psv ? e1[k] : e2[k], jo = psv ? e2[k] : e1[k];
     link_pcv[k] = (int)pcv_link.size();
     pcv_link.push_back(k);
     pcv_j1.push_back(e1[k]);
     pcv_j2.push_back(e2[k]);
+    pcv_jc.push_back(jc);
+    pcv_jo.push_back(jo);
+    pcv_sgn.push_back(psv ? -1.0 : 1.0);
+    pcv_psv.push_back(psv ? 1 : 0);
     pcv_off.push_back(pair_slot_of[{std::max(e1[k], e2[k]), std::min(e1[k], e2[k])}]);
-    if (node_xf[e2[k]] < 0) node_xf[e2[k]] = nxf++;
-    pcv_xf.push_back(node_xf[e2[k]]);
+    if (node_xf[jc] < 0) node_xf[jc] = nxf++;
+    pcv_xf.push_back(node_xf[jc]);
     pcv_hset.push_back(net->prv_hset[k]);
     pcv_km.push_back(net->km[k]);
   }
@@ -384,7 +393,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   std::vector<int> link_fcv(L, -1), fcv_link, fcv_j1, fcv_j2, fcv_off, fcv_xf1, fcv_xf2, vord;
   std::vector<double> fcv_qs, fcv_km;
   for (int k = 0; k < L; ++k) {
-    if (net->link_kind[k] == WDS_KIND_PRV) vord.push_back(link_pcv[k]);
+    if (link_pcv[k] >= 0) vord.push_back(link_pcv[k]);
     if (net->link_kind[k] != WDS_KIND_FCV) continue;
     if (e1[k] < 0 || e2[k] < 0)
       return fail(WDS_E_UNSUPPORTED, "wds_plan: an FCV with a setting must join two junctions");
@@ -403,7 +412,7 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   std::vector<int> cb_ptr(Nj + 1, 0), cb_idx;
   {
     std::vector<std::vector<int>> cb(Nj);
-    for (int i = 0; i < npcv; ++i) cb[pcv_j2[i]].push_back(i);
+    for (int i = 0; i < npcv; ++i) cb[pcv_jc[i]].push_back(i);
     for (int p = 0; p < Nj; ++p) {
       cb_idx.insert(cb_idx.end(), cb[p].begin(), cb[p].end());
       cb_ptr[p + 1] = (int)cb_idx.size();
@@ -483,7 +492,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
     for (int v : cb_idx) ok = ok && in(v, 0, std::max(npcv, 1));
     for (int i = 0; i < npcv; ++i)
       ok = ok && in(pcv_j1[i], 0, Nj) && in(pcv_j2[i], 0, Nj) && in(pcv_off[i], 0, nnzL) &&
-           in(pcv_xf[i], 0, std::max(nxf, 1)) && in(pcv_link[i], 0, L);
+           in(pcv_xf[i], 0, std::max(nxf, 1)) && in(pcv_link[i], 0, L) &&
+           in(pcv_jc[i], 0, Nj) && in(pcv_jo[i], 0, Nj);
     for (int f = 0; f < nfcv; ++f)
       ok = ok && in(fcv_j1[f], 0, Nj) && in(fcv_j2[f], 0, Nj) && in(fcv_off[f], 0, nnzL) &&
            in(fcv_xf1[f], -1, std::max(nxf, 1)) && in(fcv_xf2[f], -1, std::max(nxf, 1)) &&
@@ -531,7 +541,9 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       const int k = inc[e];
       const int other = e < inc_split[p] ? e2[k] : e1[k];
       uint32_t v = (uint32_t)k;
-      if (net->link_kind[k] == WDS_KIND_PRV || net->link_kind[k] == WDS_KIND_FCV) v |= 1u << 16;
+      if (net->link_kind[k] == WDS_KIND_PRV || net->link_kind[k] == WDS_KIND_FCV ||
+          net->link_kind[k] == WDS_KIND_PSV)
+        v |= 1u << 16;
       if (other < 0) v |= (1u << 17) | ((uint32_t)(-other - 1) << 18);
       s_in[e] = v;
     }
@@ -541,7 +553,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   std::vector<uint16_t> s_pl(pair_link.size());
   for (size_t e = 0; e < pair_link.size(); ++e)
     s_pl[e] = (uint16_t)(pair_link[e] | ((net->link_kind[pair_link[e]] == WDS_KIND_PRV ||
-                                          net->link_kind[pair_link[e]] == WDS_KIND_FCV) ? 0x8000 : 0));
+                                          net->link_kind[pair_link[e]] == WDS_KIND_FCV ||
+                                          net->link_kind[pair_link[e]] == WDS_KIND_PSV) ? 0x8000 : 0));
   if (s_pl.empty()) s_pl.push_back(0);
   struct TabOff { int sp, fp, cp, ri, lp, rp, re, md, ip, is, in, e1, e2, pp, pl, ps, fl, ds; };
   auto pack = [&](auto tag, Blob& sb, TabOff& o) {
@@ -636,7 +649,9 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
          o_lpu = blob.add(link_pump), o_phu = blob.add(phu), o_lfc = blob.add(link_fcv),
          o_fcl = blob.add(fcv_link), o_fj1 = blob.add(fcv_j1), o_fj2 = blob.add(fcv_j2),
          o_fof = blob.add(fcv_off), o_fx1 = blob.add(fcv_xf1), o_fx2 = blob.add(fcv_xf2),
-         o_fqs = blob.add(fcv_qs), o_fkm = blob.add(fcv_km), o_vord = blob.add(vord);
+         o_fqs = blob.add(fcv_qs), o_fkm = blob.add(fcv_km), o_vord = blob.add(vord),
+         o_pjc = blob.add(pcv_jc), o_pjo = blob.add(pcv_jo), o_psg = blob.add(pcv_sgn),
+         o_pps = blob.add(pcv_psv);
   WdsPlan* plan = new WdsPlan();
   if (cudaMalloc(&plan->dtab, blob.bytes.size()) != cudaSuccess) {
     delete plan;
@@ -664,6 +679,8 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   d.fcv_j1 = P_(int, o_fj1); d.fcv_j2 = P_(int, o_fj2); d.fcv_off = P_(int, o_fof);
   d.fcv_xf1 = P_(int, o_fx1); d.fcv_xf2 = P_(int, o_fx2); d.fcv_qs = P_(double, o_fqs);
   d.fcv_km = P_(double, o_fkm); d.vord = P_(int, o_vord);
+  d.pcv_jc = P_(int, o_pjc); d.pcv_jo = P_(int, o_pjo); d.pcv_sgn = P_(double, o_psg);
+  d.pcv_psv = P_(int, o_pps);
   d.cx = P_(double, o_cx); d.cy = P_(double, o_cy); d.link_tl = P_(int, o_ltl);
   d.link_pcv = P_(int, o_lpcv); d.jnode = P_(int, o_jn); d.el = P_(double, o_el);
   d.inc_ptr = P_(int, o_incp); d.inc_split = P_(int, o_incs); d.inc = P_(int, o_inc);

@@ -194,7 +194,7 @@ class GGASolver:
         self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
         lt = np.asarray(net.link_type, dtype=np.int64)
         nt = np.asarray(net.node_type, dtype=np.int64)
-        allowed = ({CVPIPE, PIPE, TCV, PUMP, PRV, FCV} if self.dense_status_machine
+        allowed = ({CVPIPE, PIPE, TCV, PUMP, PRV, PSV, FCV} if self.dense_status_machine
                    else {PIPE, TCV, PUMP})
         bad = set(lt.tolist()) - allowed
         if bad:
@@ -311,9 +311,13 @@ class GGASolver:
         kind[lt == TCV] = _lib.KIND_TCV
         kind[is_pump] = _lib.KIND_PUMP
         prv = lt == PRV
-        pcv = prv & (K0 != MISSING)
-        kind[prv & ~pcv] = _lib.KIND_PRV_FIXED
-        kind[pcv] = _lib.KIND_PRV
+        psv = lt == PSV
+        prvs = prv & (K0 != MISSING)
+        psvs = psv & (K0 != MISSING)
+        pcv = prvs | psvs             # pressure control valves with a setting
+        kind[(prv | psv) & ~pcv] = _lib.KIND_PRV_FIXED
+        kind[prvs] = _lib.KIND_PRV
+        kind[psvs] = _lib.KIND_PSV
         # FCVs with a flow setting take the valve pass and fcvstatus; a fixed
         # (MISSING setting) FCV is a fixed open/closed valve like a fixed PRV
         fcv = lt == FCV
@@ -326,16 +330,19 @@ class GGASolver:
         self.pcv_links = np.flatnonzero(pcv)
         n1 = np.asarray(net.link_n1, dtype=np.int64)
         n2 = np.asarray(net.link_n2, dtype=np.int64)
+        # the junction an ACTIVE valve holds (PRV n2, PSV n1) and its other end
+        self.pcv_jc = np.where(psvs, n1, n2)[self.pcv_links]
+        self.pcv_jo = np.where(psvs, n2, n1)[self.pcv_links]
         is_fixed = nt != 0
         if self.n_pcv:
             if self.dtype != torch.float64:
                 raise NotImplementedError(
-                    "mode=dense with setting PRVs needs float64 (ACTIVE PRV rows "
+                    "mode=dense with setting PRVs/PSVs needs float64 (ACTIVE valve rows "
                     "carry a 1e8 penalty diagonal)")
             badp = self.pcv_links[is_fixed[n1[self.pcv_links]] | is_fixed[n2[self.pcv_links]]]
             if badp.size:
                 raise NotImplementedError(
-                    "mode=dense batched PRVs need junctions at both ends: %s"
+                    "mode=dense batched PRVs/PSVs need junctions at both ends: %s"
                     % [net.link_id[int(k)] for k in badp])
         if self.fcv_links.size:
             badf = self.fcv_links[is_fixed[n1[self.fcv_links]] | is_fixed[n2[self.fcv_links]]]
@@ -344,9 +351,11 @@ class GGASolver:
                     "mode=dense batched FCVs need junctions at both ends: %s"
                     % [net.link_id[int(k)] for k in badf])
         elev = np.asarray(net.elev_ft, dtype=np.float64)
-        # valve settings: PRV head El[n2] + setting (ft), FCV flow setting (cfs)
+        # valve settings: PRV head El[n2] + setting, PSV El[n1] + setting (ft),
+        # FCV flow setting (cfs)
         prv_hset = np.zeros(L)
-        prv_hset[pcv] = elev[n2[pcv]] + K0[pcv]
+        prv_hset[prvs] = elev[n2[prvs]] + K0[prvs]
+        prv_hset[psvs] = elev[n1[psvs]] + K0[psvs]
         prv_hset[fcvs] = K0[fcvs]
         # initial flows (hydraul.c initlinkflow as restated in solver.py:2163-2174)
         q = PI * diam ** 2 / 4.0
@@ -514,9 +523,9 @@ class GGASolver:
             if self.has_cv and not status_machine:
                 raise NotImplementedError(
                     "this network has CVPIPEs: solve(..., status_machine=True) is required")
-            if self.n_pcv and not status_machine:
+            if (self.n_pcv or self.fcv_links.size) and not status_machine:
                 raise NotImplementedError(
-                    "this network has PRVs with a setting: solve(..., "
+                    "this network has PRVs/PSVs/FCVs with a setting: solve(..., "
                     "status_machine=True) is required")
         if record_schedule:
             raise NotImplementedError("record_schedule is not provided by the sm100 route")

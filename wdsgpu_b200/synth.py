@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .net import (JUNCTION, RESERVOIR, TANK, PIPE, PRV, PUMP, TCV, FCV,
+from .net import (JUNCTION, RESERVOIR, TANK, PIPE, PRV, PSV, PUMP, TCV, FCV,
                   LPSperCFS, MperFT, Net)
 
 _M3S_PER_CFS = LPSperCFS / 1000.0        # 0.028317 m3/s per cfs
@@ -571,6 +571,29 @@ def fcv_network(seed=5, links=(62, 22), settings_lps=(14.0, 70.0), km=0.5):
         st[k] = 2
         vs[k] = q
         kmi[k] = 0.02517 * km / (d[k] ** 2 * d[k] ** 2)
+    f["link_type"] = lt.astype(np.int8)
+    f["init_status"] = st.astype(np.int8)
+    f["valve_setting_user"] = vs
+    f["km_int"] = kmi
+    return Net(**f)
+
+
+def psv_network(seed=5, link=27, setting_m=72.0, km=0.5):
+    """The feature network (with its ACTIVE PRV) plus a pressure sustaining
+    valve on a junction-to-junction pipe whose upstream pressure (about 70 m)
+    lies below the valve's setting: the PSV throttles (ACTIVE) to hold its
+    upstream head at El[n1] + setting.  Link orientation follows the flow."""
+    net = feature_network(seed=seed)
+    f = net.as_fields()
+    lt = np.asarray(net.link_type).copy()
+    st = np.asarray(net.init_status).copy()
+    vs = np.asarray(net.valve_setting_user, dtype=np.float64).copy()
+    kmi = np.asarray(net.km_int, dtype=np.float64).copy()
+    d = np.asarray(net.diam_ft, dtype=np.float64)
+    lt[link] = PSV
+    st[link] = 2
+    vs[link] = setting_m
+    kmi[link] = 0.02517 * km / (d[link] ** 2 * d[link] ** 2)
     f["link_type"] = lt.astype(np.int8)
     f["init_status"] = st.astype(np.int8)
     f["valve_setting_user"] = vs
