@@ -22,6 +22,7 @@ Usage:  python tests/golden/make_golden.py        (steady cases)
                                                    and chp_ref.npz)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
         python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
+        python tests/golden/make_golden.py unrolled (unrolled-K gradient pin, unrolled_ref.npz)
 """
 import json
 import os
@@ -417,6 +418,50 @@ def make_psv():
     _valve_case(dgga, torch, net, d, rh, np.flatnonzero((lt == 3) | (lt == 4)), "psv_ref")
 
 
+def make_unrolled():
+    """Unrolled-K pin: the reference's solve_unrolled (dgga/autodiff.py:
+    1357-1664, K = 8 fixed GGA iterations, statuses frozen at the initial
+    configuration, dense mode) and its autograd gradients w.r.t. demand,
+    reservoir/tank heads, emitter Ke and pipe resistance, for L = sum of
+    squared sensor heads + squared pump flows + squared emitter flows."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.unrolled_network()
+    d, _ = synth.config2_scenarios(net, 3, seed=41, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    ke = np.broadcast_to(np.asarray(net.node_ke, dtype=np.float64), d.shape).copy()
+    sens = synth.sensor_nodes(net, 6)
+    pl = np.asarray(net.pump_link, dtype=np.int64)
+    emn = np.flatnonzero(np.asarray(net.node_ke) > 0)
+    K = 8
+    ref_net = dgga.parse.Net(**net.as_fields())
+    # dense_status_machine=True admits the check-valve pipe; solve_unrolled
+    # itself freezes the statuses at the initial configuration
+    sd = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
+    D = torch.tensor(d).requires_grad_(True)
+    RH = torch.tensor(rh).requires_grad_(True)
+    KE = torch.tensor(ke).requires_grad_(True)
+    R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+    out = dgga.autodiff.solve_unrolled(sd, D, RH, ke=KE, r_hw=R, K=K)
+    h, q, e = out["head_ft"], out["flow_cfs"], out["emitter_cfs"]
+    loss = (h[:, sens] ** 2).sum() + (q[:, pl] ** 2).sum() + (e[:, emn] ** 2).sum()
+    loss.backward()
+    blob = pack_net(net)
+    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
+                 "in_K": np.array(K)})
+    res = dict(head=h.detach().numpy(), flow=q.detach().numpy(), emitter=e.detach().numpy(),
+               g_demand=D.grad.numpy(), g_res_head=RH.grad.numpy(), g_ke=KE.grad.numpy(),
+               g_rhw=R.grad.numpy())
+    blob.update({"ref_" + k: v for k, v in res.items()})
+    path = os.path.join(HERE, "unrolled_ref.npz")
+    np.savez_compressed(path, **blob)
+    print("unrolled: K=%d, max |g_demand| %.3g -> %s" % (K, np.abs(res["g_demand"]).max(),
+                                                         os.path.basename(path)))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["eps"]:
         make_eps()
@@ -428,5 +473,7 @@ if __name__ == "__main__":
         make_fcv()
     elif sys.argv[1:] == ["psv"]:
         make_psv()
+    elif sys.argv[1:] == ["unrolled"]:
+        make_unrolled()
     else:
         main()

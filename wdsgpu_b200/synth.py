@@ -601,6 +601,32 @@ def psv_network(seed=5, link=27, setting_m=72.0, km=0.5):
     return Net(**f)
 
 
+def unrolled_network(seed=5):
+    """The feature network with its PRVs and its no-curve pump turned into
+    open pipes: power-function, custom-curve and constant-horsepower pumps,
+    TCVs, a check-valve pipe, a closed pipe, a tank as a fixed head and
+    emitters, and no control valve (the elements of the unrolled-K route; a
+    no-curve pump makes the reference's unrolled autograd return NaN, its
+    unselected power-function branch dividing by a zero slope)."""
+    net = feature_network(seed=seed, with_chp=True)
+    f = net.as_fields()
+    lt = np.asarray(net.link_type).copy()
+    st = np.asarray(net.init_status).copy()
+    prv = lt == PRV
+    lt[prv] = PIPE
+    st[prv] = 1
+    keep = np.asarray(net.pump_ptype) != 3
+    lt[np.asarray(net.pump_link)[~keep]] = PIPE
+    for key in ("pump_link", "pump_ptype", "pump_h0", "pump_r", "pump_n", "pump_q0",
+                "pump_qmax", "pump_hmax", "pump_upat"):
+        f[key] = np.asarray(f[key])[keep]
+    ptr = np.asarray(net.pump_curve_ptr)
+    f["pump_curve_ptr"] = np.concatenate([ptr[:1], ptr[1:][keep]]).astype(np.int32)
+    f["link_type"] = lt.astype(np.int8)
+    f["init_status"] = st.astype(np.int8)
+    return Net(**f)
+
+
 def config5_network(seed=5, tank_center_ft=None):
     """Extended-period workload shape: about 20 000 junctions and 23 000
     pipes, 4 power-function pumps (shutoff 40-60 m, exponent 1.85),
