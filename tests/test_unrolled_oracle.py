@@ -60,17 +60,17 @@ def test_oracle_unrolled_central_difference():
         o, _ = u.forward(dd, rh, r=rr, K=K)
         return unrolled_loss_adjoints(net, inp, o)[3][0]
 
+    # the K-iteration map is smooth only down to its rounding (about 1e-7 of
+    # the loss after 8 unconverged iterations on a matrix with a 1e8 penalty),
+    # so the steps are large: 1e-3 cfs of demand, 1e-3 of a resistance
     junc = np.flatnonzero(np.asarray(net.node_type) == 0)
     for p in junc[[3, 17, 40]]:
-        eps = 1e-6
+        eps = 1e-3
         dp, dm = d.copy(), d.copy()
         dp[0, p] += eps
         dm[0, p] -= eps
         fd = (loss(dp) - loss(dm)) / (2 * eps)
-        assert abs(fd - gd[0, p]) <= 1e-5 * max(abs(gd[0, p]), 1.0), (p, fd, gd[0, p])
-    # the K-iteration map is smooth only down to its rounding (about 1e-8 of
-    # the loss after 8 unconverged iterations), so the resistance steps are
-    # 1e-3 relative, on the pipes with the largest gradients
+        assert abs(fd - gd[0, p]) <= 2e-3 * abs(gd[0, p]), (p, fd, gd[0, p])
     r0 = np.asarray(net.r_hw, dtype=np.float64)
     for k in np.argsort(-np.abs(gr[0]))[:2]:
         eps = 1e-3 * r0[k]
