@@ -165,6 +165,13 @@ typedef struct WdsForwardOpts {
    * test) and 0 at tighter accuracies.  Polish and adjoint solves always
    * refine. */
   double refine_band;
+  /* Unrolled-K mode (solve_unrolled, dgga/autodiff.py:1357-1664): a device
+   * array [B][max_iter][L + 2 Nj] or NULL.  When set, the call runs exactly
+   * max_iter GGA iterations with no convergence test (status_machine must be
+   * 0 and polish_steps < 0, the statuses stay the initial ones) and records
+   * each iteration's starting flows, emitter flows (by junction) and
+   * solved junction heads there, for wds_unrolled_adjoint. */
+  double* unroll_record;
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;
@@ -207,6 +214,22 @@ int wds_adjoint_pumps(WdsPlan* plan, int32_t batch, const double* gH,
                       const double* gQ, const double* gE, double* gd, double* grh,
                       double* gke, double* gr, double* gspeed, double* gh0, double* grp,
                       void* stream);
+
+/* Gradient of the unrolled-K map (solve_unrolled, dgga/autodiff.py:
+ * 1357-1664, differentiated there by torch autograd): after a wds_forward
+ * with opts.unroll_record = record and max_iter = K, the reverse pass over
+ * the K iterations maps the output adjoints gH [B,N], gQ [B,L], gE [B,N] to
+ * gd, grh, gke [B,N] and gr [B,L] (per scenario; a shared parameter takes
+ * the batch sum).  demand / fixed_head / ke / r are the forward's inputs.
+ * scratch: device array [B][2 L + 2 Nj].  Networks with control valves
+ * (PRV/PSV/FCV with a setting) are refused, as by the reference.  Rebuilds
+ * each iteration's factor in the plan's workspace, so a kept implicit state
+ * is gone afterwards. */
+int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K, const double* record,
+                         const double* demand, const double* fixed_head, const double* ke,
+                         int64_t ke_stride, const double* r, int64_t r_stride,
+                         const double* gH, const double* gQ, const double* gE, double* gd,
+                         double* grh, double* gke, double* gr, double* scratch, void* stream);
 
 /* Statistics of the plan: [Nj, nnz_L, n_levels, n_pairs, smem_bytes,
  * n_pcv, nnz_A_lower, threads]. */

@@ -143,3 +143,21 @@ def test_pump_rows_host_rules():
     with pytest.raises(NotImplementedError):                         # frozen status
         implicit_solve(s, net.demand_cfs_at(0), net.fixed_head_ft_at(0),
                        status=np.zeros(s.L, dtype=np.int8))
+
+
+def test_unrolled_host_rules():
+    """solve_unrolled refuses what the reference refuses (control valves) and
+    what this route does not take (warm starts, a frozen status, pump
+    parameters); the health probe checks its parameter name."""
+    from wdsgpu_b200.autodiff import solve_unrolled, unrolled_grad_health
+    s = GGASolver(synth.config2_network(), device="cpu", dense_status_machine=True)
+    d, rh = s.net.demand_cfs_at(0), s.net.reservoir_head_ft_at(0)
+    with pytest.raises(NotImplementedError):          # PRVs with a setting
+        solve_unrolled(s, d, rh, K=3)
+    s2 = GGASolver(synth.unrolled_network(), device="cpu", dense_status_machine=True)
+    with pytest.raises(NotImplementedError):
+        solve_unrolled(s2, d, rh, K=3, status=np.zeros(s2.L, dtype=np.int8))
+    with pytest.raises(ValueError):
+        solve_unrolled(s2, d, rh, K=3, assemble="dense")
+    with pytest.raises(ValueError):
+        unrolled_grad_health(s2, d, rh, param="speed")

@@ -25,7 +25,8 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
            "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc",
-           "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs", "wds_adjoint_pumps")
+           "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs", "wds_adjoint_pumps",
+           "wds_unrolled_adjoint")
 MULTI_MAX = 8
 
 
@@ -65,7 +66,7 @@ class WdsForwardOpts(ctypes.Structure):
         ("r_stride", ctypes.c_int64), ("q0", ctypes.c_void_p), ("e0", ctypes.c_void_p),
         ("pump_speed", ctypes.c_void_p), ("pump_h0", ctypes.c_void_p),
         ("pump_r", ctypes.c_void_p), ("pump_stride", ctypes.c_int64),
-        ("refine_band", ctypes.c_double),
+        ("refine_band", ctypes.c_double), ("unroll_record", ctypes.c_void_p),
     ]
 
 
@@ -113,6 +114,9 @@ def load():
     lib.wds_adjoint_rhs.restype = ctypes.c_int
     lib.wds_adjoint_pumps.argtypes = [vp, ctypes.c_int32] + [vp] * 10 + [vp]
     lib.wds_adjoint_pumps.restype = ctypes.c_int
+    lib.wds_unrolled_adjoint.argtypes = [vp, ctypes.c_int32, ctypes.c_int32] + [vp] * 4 + \
+        [ctypes.c_int64, vp, ctypes.c_int64] + [vp] * 8 + [vp]
+    lib.wds_unrolled_adjoint.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]
     lib.wds_plan_stats.restype = ctypes.c_int
     lib.wds_plan_symbolic.argtypes = [vp] + [c_int32_p] * 5

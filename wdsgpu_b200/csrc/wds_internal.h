@@ -158,6 +158,7 @@ struct FwdArgs {
   const double* rh;
   const double* ke;
   const double* r;
+  double* rec;       // unrolled record [B][K][L + 2 Nj] (q, e, H per iteration) or null
   const double* q0;  // [B][L] warm-start flows or null
   const double* e0;  // [B][N] warm-start emitter flows or null
   // pump parameters of the call ([L] rows, stride 0 or L; null: the network's)
@@ -202,6 +203,27 @@ struct HostSym {
 
 // Kernels run `groups` independent scenario groups of 256 threads per CTA;
 // shared memory = schedule tables + groups * per-scenario state.
+// Reverse pass of the unrolled-K map (wds_unrolled_adjoint)
+struct UnrollArgs {
+  int B, K;
+  const double* rec;    // [B][K][L + 2 Nj] from the unrolled forward
+  const double* d;      // [B][N]
+  const double* rh;     // [B][N]
+  const double* ke;
+  long long ke_stride;
+  const double* r;
+  long long r_stride;
+  const double* gH;     // [B][N]
+  const double* gQ;     // [B][L]
+  const double* gE;     // [B][N]
+  double* gd;           // [B][N]
+  double* grh;          // [B][N]
+  double* gke;          // [B][N]
+  double* gr;           // [B][L]
+  double* scr;          // [B][2 L + 2 Nj]
+};
+int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int groups,
+                    void* stream, std::string* err);
 int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
                    void* stream, std::string* err);
 int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int groups,

@@ -1258,7 +1258,15 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
   int nextcheck = n.checkfreq;
   int iters = maxtrials + 1, info = WDS_INFO_UNCONVERGED;
   double relerr = 0.0;
+  const int rec_w = n.L + 2 * n.Nj;  // unrolled record: q [L], e [Nj], H [Nj] per iteration
+  double* recb = a.rec ? a.rec + (size_t)b * maxtrials * rec_w : nullptr;
   for (int it = 1; it <= (em_ok ? maxtrials : 0); ++it) {
+    if (recb) {  // state at the start of iteration it, for the unrolled reverse pass
+      double* r = recb + (size_t)(it - 1) * rec_w;
+      for (int k = gtid<NT>(); k < n.L; k += NT) r[k] = s.q[k];
+      for (int p = gtid<NT>(); p < n.Nj; p += NT)
+        r[n.L + p] = s.eslot[p] >= 0 ? s.em_e[s.eslot[p]] : 0.0;
+    }
     // ---- headloss coefficients
     for (int k = gtid<NT>(); k < n.L; k += NT) {
       double P, Y;
@@ -1277,6 +1285,10 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
     // WdsForwardOpts.refine_band); relerr still holds the previous iteration's
     const bool refine_it = a.rband <= 0.0 || it > 20 || (it > 1 && relerr < a.rband);
     solve_refined<NT, FT>(n, T, s, s.V0, -1, s.V1, s.V2, refine_it ? a.refine : 0);
+    if (recb) {
+      double* r = recb + (size_t)(it - 1) * rec_w + n.L + n.Nj;
+      for (int p = gtid<NT>(); p < n.Nj; p += NT) r[p] = s.V1[p];
+    }
     // ---- newflows (hydsolver.c:358-514 as restated in solver.py:3092-3110)
     double sums[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k = gtid<NT>(); k < n.L; k += NT) {
@@ -1304,7 +1316,7 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
     const double dqsum = sums[0] + sums[2], qsum = sums[1] + sums[3];
     relerr = qsum > a.hacc ? dqsum / qsum : dqsum;
     if (!sm) {
-      if (!(relerr > a.hacc)) {
+      if (!recb && !(relerr > a.hacc)) {  // the unrolled map runs all its iterations
         iters = it;
         info = 0;
         break;
@@ -1409,6 +1421,10 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
       info = 0;
       break;
     }
+  }
+  if (recb && em_ok && info == WDS_INFO_UNCONVERGED) {  // K iterations done
+    iters = maxtrials;
+    info = 0;
   }
   gsync<NT>();
   // junction heads of the GGA solution stay in V1
@@ -1761,6 +1777,296 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
   }
 }
 
+// ---------------------------------------------------------------- unrolled-K reverse
+// dP/dq, dY/dq, dP/dr, dY/dr of one link on the branch its coefficients took
+// (the formulas of solve_unrolled, dgga/autodiff.py:1495-1591, differentiated
+// as autograd does: a clamped quantity is a constant, |q| is q sgn with sgn
+// constant; a custom pump curve's segment is chosen from the detached flow).
+__device__ void link_dcoef(const DevNet& n, int k, double q, int st, double r, double& Pq,
+                           double& Yq, double& Pr, double& Yr) {
+  Pq = Yq = Pr = Yr = 0.0;
+  const int kd = n.kind[k];
+  if (st <= WDS_CLOSED || (n.flags[k] & WDS_F_ZERO_SPEED)) {  // P = 1/CBIG, Y = q
+    Yq = 1.0;
+    return;
+  }
+  const double sgn = q < 0.0 ? -1.0 : 1.0, qa = q * sgn;
+  double hg, hl, dhg, dhl;
+  if (kd <= WDS_KIND_CVPIPE) {
+    const double ex = n.hexp, qc = fmax(qa, 1e-30);
+    const double hg0 = ex * r * pow(qc, ex - 1.0);
+    const bool lin = hg0 < n.rqtol;
+    hg = lin ? n.rqtol : hg0;
+    hl = lin ? hg * qa : hg * qa / ex;
+    dhg = (lin || !(qa > 1e-30)) ? 0.0 : ex * (ex - 1.0) * r * pow(qc, ex - 2.0);
+    dhl = lin ? n.rqtol : dhg * qa / ex + hg / ex;
+    const double dhg_r = lin ? 0.0 : ex * pow(qc, ex - 1.0);
+    const double dhl_r = dhg_r * qa / ex;
+    const double km = n.km[k];
+    if (km > 0.0) {
+      hl += km * qa * qa;
+      dhl += 2.0 * km * qa;
+      hg += 2.0 * km * qa;
+      dhg += 2.0 * km;
+    }
+    Pq = -dhg * sgn / (hg * hg);
+    Yq = (dhl * hg - hl * dhg) / (hg * hg);
+    Pr = -dhg_r / (hg * hg);
+    Yr = sgn * (dhl_r * hg - hl * dhg_r) / (hg * hg);
+    return;
+  }
+  if (kd == WDS_KIND_TCV) {
+    const double km = n.km_tcv[k];
+    if (!(km > 0.0)) {
+      Yq = 1.0;
+      return;
+    }
+    const double hg0 = 2.0 * km * qa;
+    const bool lin = hg0 < n.rqtol;
+    hg = lin ? n.rqtol : hg0;
+    dhg = lin ? 0.0 : 2.0 * km * sgn;
+    hl = lin ? q * hg : q * hg / 2.0;
+    dhl = lin ? hg : (hg + q * dhg) / 2.0;
+    Pq = -dhg / (hg * hg);
+    Yq = (dhl * hg - hl * dhg) / (hg * hg);
+    return;
+  }
+  if (kd != WDS_KIND_PUMP) return;
+  const int t = n.ptype[k];
+  if (t == 3) {  // NOCURVE: P const, Y = q
+    Yq = 1.0;
+    return;
+  }
+  const double spc = fmax(n.pspeed[k], 1e-12);
+  if (t == 2) {  // CUSTOM, segment frozen: hg const, hl = H0 w^2 + hg q
+    Yq = 1.0;
+    return;
+  }
+  const double pn = n.pn[k];
+  const double h0e = spc * spc * n.ph0[k];
+  const double re = n.pr[k] * pow(spc, 2.0 - pn);
+  if (t == 0) {  // CONST_HP
+    const double qa2 = fmax(qa * qa, 1e-30);
+    const double raw = -re / qa2;
+    const bool big = raw > kCBIG, sml = raw < n.rqtol;
+    hg = big ? kCBIG : (sml ? n.rqtol : raw);
+    dhg = (big || sml || !(qa * qa >= 1e-30)) ? 0.0 : 2.0 * re / (qa2 * qa2) * qa * sgn;
+    const double qcc = sgn * fmax(qa, 1e-30);
+    hl = (big || sml) ? -hg * q : re / qcc;
+    dhl = (big || sml) ? -hg : (qa > 1e-30 ? -re / (qcc * qcc) : 0.0);
+  } else if (pn == 1.0) {  // linear
+    hg = re;
+    dhg = 0.0;
+    hl = h0e + re * q;
+    dhl = re;
+  } else {  // power function
+    const double qc = fmax(qa, 1e-30);
+    const double raw = pn * re * pow(qc, pn - 1.0);
+    const bool sml = raw < n.rqtol;
+    hg = sml ? n.rqtol : raw;
+    dhg = (sml || !(qa > 1e-30)) ? 0.0 : pn * (pn - 1.0) * re * pow(qc, pn - 2.0) * sgn;
+    const double nn = fmax(pn, 1e-30);
+    hl = sml ? h0e + hg * q : h0e + hg * q / nn;
+    dhl = sml ? hg : (dhg * q + hg) / nn;
+  }
+  Pq = -dhg / (hg * hg);
+  Yq = (dhl * hg - hl * dhg) / (hg * hg);
+}
+
+// Derivatives of an emitter's hloss and hgrad in its flow e and its Ke.
+__device__ __forceinline__ void emitter_dcoef(const DevNet& n, double e, double ke, double hge,
+                                              double& hle_e, double& hge_e, double& hle_k,
+                                              double& hge_k) {
+  const double kea = fmax(ke, kCSMALL), dkea = ke > kCSMALL ? 1.0 : 0.0;
+  const double ae = fabs(e), ea = fmax(ae, 1e-30);
+  const double sg = e > 0.0 ? 1.0 : (e < 0.0 ? -1.0 : 0.0);
+  const bool lin = n.qexp * kea * pow(ea, n.qexp - 1.0) < n.rqtol;
+  hge_e = (lin || !(ae > 1e-30)) ? 0.0 : n.qexp * (n.qexp - 1.0) * kea * pow(ea, n.qexp - 2.0) * sg;
+  hge_k = lin ? 0.0 : n.qexp * pow(ea, n.qexp - 1.0) * dkea;
+  hle_e = lin ? n.rqtol : (hge_e * e + hge) / n.qexp;
+  hle_k = lin ? 0.0 : hge_k * e / n.qexp;
+}
+
+// Reverse pass of the unrolled-K map (solve_unrolled's autograd,
+// dgga/autodiff.py:1357-1664) for one scenario group.  From the record of the
+// forward, iteration k's coefficients, node matrix and factor are rebuilt
+// (the same functions as the forward), then:
+//   q' = q - (Y - P dh): qb -> Yb, Pb, dh_b (or qb / 2 on the constant-HP half step)
+//   e' = e - (hle - (H - el)) / hge: eb -> hle_b, hge_b, H_b
+//   H = A^{-1} F:       Fb = A^{-1} H_b (A symmetric), Pb -= (Fb1 - Fb2)(H1 - H2)
+//   F = Y terms + P H_fixed + emitter terms + Xflow(q, e, d)
+// and the coefficients' derivatives carry Pb, Yb, hle_b, hge_b to the flows,
+// emitter flows, resistances and Ke.  Node sums gather over the incidence
+// lists (no atomics).  Scratch per scenario: qb [L], a link temporary [L],
+// eb [Nj], Fb [Nj].
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void unrolled_body(const DevNet& n, const DevWork& w, const UnrollArgs& u,
+                                              int state_bytes, int blk, int groups) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int g = threadIdx.x / NT;
+  const int b = blk * groups + g;
+  TB T;
+  Sh s;
+  if constexpr (TB::kWide) {
+    if (g >= groups || b >= u.B) return;
+    T = tab_view<TB>(n, (const unsigned char*)n.stab);
+    s = carve(n, w.state + (size_t)b * state_bytes);
+  } else {
+    for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
+      ((uint4*)smem_raw)[i] = n.stab[i];
+    __syncthreads();
+    T = tab_view<TB>(n, smem_raw);
+    if (g >= groups || b >= u.B) return;
+    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+  }
+  const int tid = gtid<NT>();
+  s.q = w.lk + (size_t)b * 2 * n.L;
+  s.Y = s.q + n.L;
+  s.Mg = w.M + (size_t)b * n.nT * n.nT;
+  const double* rrow = u.r + (long long)b * u.r_stride;
+  const double* kerow = u.ke + (long long)b * u.ke_stride;
+  const double* drow = u.d + (size_t)b * n.N;
+  const double* rhrow = u.rh + (size_t)b * n.N;
+  FwdArgs a0{};  // the network's own pump parameters
+  const PumpTh th = pump_th(n, a0, b);
+  for (int f = tid; f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
+  for (int k = tid; k < n.L; k += NT) s.S[k] = n.status0[k];
+  gsync<NT>();
+  if (!build_emitters<NT>(n, s, kerow, 1)) return;  // uniform; the forward failed alike
+  double* qb = u.scr + (size_t)b * (2 * n.L + 2 * n.Nj);
+  double* tl = qb + n.L;
+  double* eb = tl + n.L;
+  double* Fb = eb + n.Nj;
+  double* gd = u.gd + (size_t)b * n.N;
+  double* grh = u.grh + (size_t)b * n.N;
+  double* gke = u.gke + (size_t)b * n.N;
+  double* gr = u.gr + (size_t)b * n.L;
+  const double* gH = u.gH + (size_t)b * n.N;
+  for (int i = tid; i < n.N; i += NT) {
+    gd[i] = 0.0;
+    grh[i] = 0.0;
+    gke[i] = 0.0;
+  }
+  for (int k = tid; k < n.L; k += NT) {
+    gr[k] = 0.0;
+    qb[k] = u.gQ[(size_t)b * n.L + k];
+  }
+  for (int p = tid; p < n.Nj; p += NT)
+    eb[p] = s.eslot[p] >= 0 ? u.gE[(size_t)b * n.N + n.jnode[p]] : 0.0;
+  gsync<NT>();
+  const int R = n.L + 2 * n.Nj;
+  const double* recb = u.rec + (size_t)b * u.K * R;
+  for (int kk = u.K - 1; kk >= 0; --kk) {
+    const double* rr = recb + (size_t)kk * R;
+    const bool last = kk == u.K - 1;
+    for (int k = tid; k < n.L; k += NT) s.q[k] = rr[k];
+    for (int p = tid; p < n.Nj; p += NT) {
+      const int es = s.eslot[p];
+      if (es >= 0) s.em_e[es] = rr[n.L + p];
+      s.V1[p] = rr[n.L + n.Nj + p];
+    }
+    gsync<NT>();
+    for (int k = tid; k < n.L; k += NT) {
+      double P, Y;
+      link_coef(n, th, k, s.q[k], s.S[k], rrow[k], false, P, Y);
+      s.P[k] = P;
+      s.Y[k] = Y;
+    }
+    gsync<NT>();
+    assemble_gga<NT, FT>(n, T, s, kerow, drow);
+    factor<NT, FT>(n, T, s);  // the forward factored this matrix: positive definite
+    // (1) q' = q - dq: the head-difference adjoint of each link
+    for (int k = tid; k < n.L; k += NT) {
+      const double dh = head_of(T.e1[k], s.V1, s.hf) - head_of(T.e2[k], s.V1, s.hf);
+      const double dq = s.Y[k] - s.P[k] * dh;
+      const bool hit = (n.flags[k] & WDS_F_CHP) && dq > s.q[k];
+      tl[k] = hit ? 0.0 : qb[k] * s.P[k];
+    }
+    gsync<NT>();
+    // (2) H_b at the junctions (links, emitter update, output) -> V0; fixed heads -> grh
+    for (int p = tid; p < n.Nj; p += NT) {
+      double acc = 0.0;
+      const int a = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
+      for (int e = a; e < m; ++e) acc += tl[inc_link(T, e)];
+      for (int e = m; e < z; ++e) acc += -tl[inc_link(T, e)];
+      if (last) acc += gH[n.jnode[p]];
+      const int es = s.eslot[p];
+      if (es >= 0) {
+        double hle, hge;
+        emitter_hl(n, s.em_e[es], s.em_ke[es], hle, hge);
+        acc += eb[p] / hge;  // e' = e - (hle - (H - el)) / hge: de'/dH = 1/hge
+      }
+      s.V0[p] = acc;
+    }
+    for (int f = tid; f < n.Nf; f += NT) {
+      double acc = 0.0;
+      for (int e = n.finc_ptr[f]; e < n.finc_split[f]; ++e) acc += tl[n.finc[e]];
+      for (int e = n.finc_split[f]; e < n.finc_ptr[f + 1]; ++e) acc += -tl[n.finc[e]];
+      if (last) acc += gH[n.fnode[f]];
+      grh[n.fnode[f]] += acc;
+    }
+    gsync<NT>();
+    // (3) F_b = A^{-1} H_b
+    solve_refined<NT, FT>(n, T, s, s.V0, -1, Fb, s.V2, 2);
+    // (4) links: P_b, Y_b from q', A and F; carried to q and r
+    for (int k = tid; k < n.L; k += NT) {
+      const double q = s.q[k], P = s.P[k], Y = s.Y[k];
+      const int c1 = T.e1[k], c2 = T.e2[k];
+      const double dh = head_of(c1, s.V1, s.hf) - head_of(c2, s.V1, s.hf);
+      const bool hit = (n.flags[k] & WDS_F_CHP) && (Y - P * dh) > q;
+      const double dqb = -qb[k];
+      const double uu = junc_of(c1, Fb) - junc_of(c2, Fb);
+      const double vv = junc_of(c1, s.V1) - junc_of(c2, s.V1);
+      double Pb = (hit ? 0.0 : -dqb * dh) - uu * vv;
+      const double Yb = (hit ? 0.0 : dqb) + uu;
+      double tg = 0.0;  // F = ... + P H_fixed at the junction end
+      if (c1 < 0 && c2 >= 0) {
+        Pb += Fb[c2] * s.hf[-c1 - 1];
+        tg = Fb[c2] * P;
+      } else if (c2 < 0 && c1 >= 0) {
+        Pb += Fb[c1] * s.hf[-c2 - 1];
+        tg = Fb[c1] * P;
+      }
+      tl[k] = tg;
+      double Pq, Yq, Pr, Yr;
+      link_dcoef(n, k, q, s.S[k], rrow[k], Pq, Yq, Pr, Yr);
+      qb[k] = qb[k] + (hit ? dqb / 2.0 : 0.0) - uu + Pb * Pq + Yb * Yq;
+      gr[k] += Pb * Pr + Yb * Yr;
+    }
+    gsync<NT>();
+    // (5) fixed heads through the grounding terms; junctions: demand, emitters
+    for (int f = tid; f < n.Nf; f += NT) {
+      double acc = 0.0;
+      for (int e = n.finc_ptr[f]; e < n.finc_ptr[f + 1]; ++e) acc += tl[n.finc[e]];
+      grh[n.fnode[f]] += acc;
+    }
+    for (int p = tid; p < n.Nj; p += NT) {
+      const double Fp = Fb[p];
+      gd[n.jnode[p]] += -Fp;
+      const int es = s.eslot[p];
+      if (es < 0) continue;
+      const double ee = s.em_e[es], ke = s.em_ke[es];
+      double hle, hge, hle_e, hge_e, hle_k, hge_k;
+      emitter_hl(n, ee, ke, hle, hge);
+      emitter_dcoef(n, ee, ke, hge, hle_e, hge_e, hle_k, hge_k);
+      const double dqe = (hle - (s.V1[p] - n.el[p])) / hge;
+      const double dqeb = -eb[p];
+      const double hleb = dqeb / hge + Fp / hge;
+      const double hgeb = -dqeb * dqe / hge + Fp * s.V1[p] / (hge * hge) -
+                          Fp * (hle + n.el[p]) / (hge * hge);
+      eb[p] = eb[p] - Fp + hleb * hle_e + hgeb * hge_e;
+      gke[n.jnode[p]] += hleb * hle_k + hgeb * hge_k;
+    }
+    gsync<NT>();
+  }
+}
+
+template <int NT, int GR, class TB, class FT>
+__global__ void __launch_bounds__(NT * GR, 1) k_unrolled(DevNet n, DevWork w, UnrollArgs u,
+                                                         int state_bytes) {
+  unrolled_body<NT, TB, FT>(n, w, u, state_bytes, blockIdx.x, GR);
+}
+
 template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
                                                         int state_bytes) {
@@ -1901,6 +2207,32 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int grou
   ce = cudaGetLastError();
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward launch: ") + cudaGetErrorString(ce);
+    return WDS_E_CUDA;
+  }
+  return WDS_OK;
+}
+
+int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int groups,
+                    void* stream, std::string* err) {
+  const int st = (int)smem_bytes(n);
+  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
+  void (*kern)(DevNet, DevWork, UnrollArgs, int) =
+      n.fp32 ? (n.wide ? k_unrolled<256, 1, LTab, float>
+                : groups == 1 ? k_unrolled<256, 1, STab, float>
+                : groups == 2 ? k_unrolled<256, 2, STab, float> : k_unrolled<256, 3, STab, float>)
+             : (n.wide ? k_unrolled<256, 1, LTab, double>
+                : groups == 1 ? k_unrolled<256, 1, STab, double>
+                : groups == 2 ? k_unrolled<256, 2, STab, double> : k_unrolled<256, 3, STab, double>);
+  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (ce != cudaSuccess) {
+    *err = std::string("wds_unrolled_adjoint: ") + cudaGetErrorString(ce);
+    return WDS_E_CUDA;
+  }
+  const int grid = (u.B + groups - 1) / groups;
+  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, u, st);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    *err = std::string("wds_unrolled_adjoint launch: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
   return WDS_OK;

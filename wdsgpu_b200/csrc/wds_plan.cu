@@ -800,6 +800,9 @@ static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::
   if (!(o->refine_band >= 0.0))
     return fail(WDS_E_ARG, who + ": refine_band must be >= 0");
   a.rband = o->refine_band;
+  a.rec = o->unroll_record;
+  if (a.rec && (o->status_machine || o->polish_steps >= 0))
+    return fail(WDS_E_ARG, who + ": the unrolled mode runs with status_machine 0 and no polish");
   a.th_sp = o->pump_speed;
   a.th_h0 = o->pump_h0;
   a.th_r = o->pump_r;
@@ -969,6 +972,35 @@ extern "C" int wds_adjoint_pumps(WdsPlan* plan, int32_t batch, const double* gH,
   a.grp = grp;
   std::string err;
   int rc = launch_adjoint(plan->dn, plan->dw, a, plan->groups, stream, &err);
+  if (rc != WDS_OK) return fail(rc, err);
+  return WDS_OK;
+}
+
+extern "C" int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K,
+                                    const double* record, const double* demand,
+                                    const double* fixed_head, const double* ke,
+                                    int64_t ke_stride, const double* r, int64_t r_stride,
+                                    const double* gH, const double* gQ, const double* gE,
+                                    double* gd, double* grh, double* gke, double* gr,
+                                    double* scratch, void* stream) {
+  using namespace wds;
+  if (!plan || batch <= 0 || K <= 0 || !record || !demand || !fixed_head || !ke || !r || !gH ||
+      !gQ || !gE || !gd || !grh || !gke || !gr || !scratch)
+    return fail(WDS_E_ARG, "wds_unrolled_adjoint: bad argument");
+  if (batch > plan->max_batch)
+    return fail(WDS_E_ARG, "wds_unrolled_adjoint: batch exceeds the plan's max_batch");
+  if (plan->dn.npcv > 0 || plan->dn.nfcv > 0)
+    return fail(WDS_E_UNSUPPORTED,
+                "wds_unrolled_adjoint: control valves (PRV/PSV/FCV) are not on the unrolled route");
+  if ((ke_stride != 0 && ke_stride != plan->dn.N) || (r_stride != 0 && r_stride != plan->dn.L))
+    return fail(WDS_E_ARG, "wds_unrolled_adjoint: ke_stride must be 0 or N, r_stride 0 or L");
+  UnrollArgs u{};
+  u.B = batch; u.K = K; u.rec = record; u.d = demand; u.rh = fixed_head; u.ke = ke;
+  u.ke_stride = ke_stride; u.r = r; u.r_stride = r_stride; u.gH = gH; u.gQ = gQ; u.gE = gE;
+  u.gd = gd; u.grh = grh; u.gke = gke; u.gr = gr; u.scr = scratch;
+  std::string err;
+  const int rc = launch_unrolled(plan->dn, plan->dw, u, plan->groups, stream, &err);
+  plan->have_state = false;  // the reverse pass reuses the plan's factor workspace
   if (rc != WDS_OK) return fail(rc, err);
   return WDS_OK;
 }

@@ -579,7 +579,8 @@ class GGASolver:
         return tuple(None if t is None else t.expand(rows, L).contiguous() for t in out)
 
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
-            refine=None, plan=None, q0=None, e0=None, pumps=None, refine_band=None):
+            refine=None, plan=None, q0=None, e0=None, pumps=None, refine_band=None,
+            record=None):
         """One wds_forward call on device tensors; returns the raw outputs.
         q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
         warm start of GGASolver.solve (dgga/solver.py:2876-2887); pumps is
@@ -600,6 +601,8 @@ class GGASolver:
         o.status_machine = 1 if status_machine else 0
         o.refine = int(self.refine_steps() if refine is None else refine)
         o.refine_band = float(self.refine_band(hacc) if refine_band is None else refine_band)
+        if record is not None:   # unrolled mode: max_iter iterations, recorded
+            o.unroll_record = record.data_ptr()
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
