@@ -148,3 +148,43 @@ def test_pumpstatus_shutoff_at_call_speed(cuda):
     _check_against_oracle(net, inp, th, h, q, gd, g)
     assert abs(q[1, pl[0]]) < 1e-5 and abs(q[0, pl[0]]) > 1e-3
     assert g[0][1, pl[0]] == 0.0 and g[0][0, pl[0]] != 0.0
+
+
+def test_clamp_branch_in_multi_and_eps_routes(cuda):
+    """The constant-HP clamp-branch correction in the multi-plan launch (the
+    same gradients as one implicit_solve per network) and in the
+    extended-period adjoint (the oracle's adjoint through time, whose steps use
+    the exact clamp Jacobian)."""
+    from wdsgpu_b200 import synth
+    from wdsgpu_b200.autodiff import implicit_solve
+    from wdsgpu_b200.eps import eps_solve
+    from wdsgpu_b200.multi import implicit_solve_multi
+    from wdsgpu_b200.solver import GGASolver
+    from oracle.eps import EpsOracle
+    nets = [load("chp_ref"), load("pump_ref")]
+    solvers = [GGASolver(net, device=cuda, dense_status_machine=True) for net, _, _ in nets]
+    Ds = [torch.tensor(inp["demand"], device=cuda).requires_grad_(True) for _, inp, _ in nets]
+    RHs = [torch.tensor(np.nan_to_num(inp["res_head"]), device=cuda) for _, inp, _ in nets]
+    outs = implicit_solve_multi(solvers, Ds, RHs, accuracy=1e-7)
+    sum((h ** 2).sum() for h, _, _ in outs).backward()
+    for s, D, RH in zip(solvers, Ds, RHs):
+        D1 = D.detach().clone().requires_grad_(True)
+        (implicit_solve(s, D1, RH, accuracy=1e-7)[0] ** 2).sum().backward()
+        G, R = D.grad.cpu().numpy(), D1.grad.cpu().numpy()
+        assert np.abs(G - R).max() <= 1e-9 * np.abs(R).max()
+    net, inp, _ = nets[0]
+    s = solvers[0]
+    T, B = 2, 2
+    dem = np.stack([inp["demand"][:B] * f for f in (1.0, 1.05)])
+    rh = np.nan_to_num(inp["res_head"][:B])
+    th0 = np.broadcast_to(np.asarray(net.tank_h0), (B, len(net.tank_node))).copy()
+    D = torch.tensor(dem, device=cuda).requires_grad_(True)
+    out = eps_solve(s, D, torch.tensor(rh, device=cuda), torch.tensor(th0, device=cuda),
+                    accuracy=1e-7)
+    (out["head"] ** 2).sum().backward()
+    eo = EpsOracle(net)
+    run = eo.run(dem, rh, th0, accuracy=1e-7)
+    g_dem = eo.backward(run, 2.0 * run["head"], np.zeros((T, B, net.L)),
+                        np.zeros((T, B, net.N)), np.zeros((T + 1, B, len(net.tank_node))))[0]
+    G = D.grad.cpu().numpy()
+    assert np.abs(G - g_dem).max() <= 1e-7 * np.abs(g_dem).max()

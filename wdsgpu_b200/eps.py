@@ -37,7 +37,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .autodiff import _adjoint_guards
+from .autodiff import _adjoint_guards, _clamp_grh, _clamp_rhs
 from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
 
 __all__ = ["eps_solve", "EpsSM100", "tank_links"]
@@ -154,7 +154,7 @@ class EpsSM100(torch.autograd.Function):
             rh[:, tk.node] = h
             o = _step_forward(s, d_all[t], rh, ke_t, r_t, B, max_iter, accuracy,
                               polish_steps, q0, e0)
-            _adjoint_guards(s, o["flow"], o["status"])
+            _adjoint_guards(s, o["flow"], o["status"], allow_clamp=True)
             heads[t], flows[t], emits[t] = o["head"], o["flow"], o["emit"]
             # checkpoint of the step: its warm start (tank heads are tank_heads[t])
             if q0 is None:
@@ -205,8 +205,16 @@ class EpsSM100(torch.autograd.Function):
             rh[:, tk.node] = tank_heads[t]
             o = _step_forward(s, d_all[t], rh, ke_t, r_t, B, max_iter, acc, polish,
                               warm_q[t].contiguous(), warm_e[t].contiguous())
-            gd, grh, gke, gr = _adjoint_launch(s, o["plan"], B, gH[t].contiguous(),
-                                               gq.contiguous(), gE[t].contiguous())
+            gHt, gq, gEt = gH[t].contiguous(), gq.contiguous(), gE[t].contiguous()
+            # constant-HP pumps on their clamp branch: Woodbury on the kept factor
+            clamp = _adjoint_guards(s, o["flow"], o["status"], allow_clamp=True)
+            fix = None
+            if clamp is not None:
+                gHt, fix = _clamp_rhs(s, o["plan"], B, clamp, gHt, gq, gEt,
+                                      torch.cuda.current_stream(dev).cuda_stream)
+            gd, grh, gke, gr = _adjoint_launch(s, o["plan"], B, gHt, gq, gEt)
+            if fix is not None:
+                _clamp_grh(fix, gq, gd, grh)
             g_dem[t] = gd
             g_rh += grh
             g_ke += gke

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .autodiff import _adjoint_guards
+from .autodiff import _adjoint_guards, _clamp_grh, _clamp_rhs
 from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
 
 __all__ = ["implicit_solve_multi", "solve_multi"]
@@ -119,7 +119,7 @@ class ImplicitMultiSM100(torch.autograd.Function):
             d_, rh_, ke_, r_, B, _ = s._inputs(d.detach(), rh.detach(), ke.detach(), r.detach())
             ins.append((d_, rh_, ke_.contiguous(), r_.contiguous(), B))
         outs, plans = _forward_multi(solvers, ins, accuracy, max_iter, True, polish_steps)
-        res = []
+        res, clamps = [], []
         for s, o in zip(solvers, outs):
             info = o["info"]
             _check_emitter_cap(s, info)
@@ -130,9 +130,9 @@ class ImplicitMultiSM100(torch.autograd.Function):
                                        "is not positive definite%s" % (bad[:8], _not_pd_hint(s)))
                 raise RuntimeError("implicit_solve_multi: scenarios %s did not converge"
                                    % bad[:8])
-            _adjoint_guards(s, o["flow"], o["status"])
+            clamps.append(_adjoint_guards(s, o["flow"], o["status"], allow_clamp=True))
             res += [o["head"], o["flow"], o["emit"]]
-        ctx.solvers, ctx.plans = solvers, plans
+        ctx.solvers, ctx.plans, ctx.clamps = solvers, plans, clamps
         ctx.B = [x[4] for x in ins]
         ctx.shapes = [(t.dim(), t.device) for t in tensors]
         return tuple(res)
@@ -145,7 +145,7 @@ class ImplicitMultiSM100(torch.autograd.Function):
         n = len(solvers)
         io = (_lib.WdsAdjointIO * n)()
         batch = (ctypes.c_int32 * n)()
-        keep, outs = [], []
+        keep, outs, fixes = [], [], []
         for p, s in enumerate(solvers):
             B, dev = ctx.B[p], s.device
 
@@ -155,6 +155,11 @@ class ImplicitMultiSM100(torch.autograd.Function):
                 return g.detach().to(torch.float64).contiguous()
 
             gH, gQ, gE = _g(grads[3 * p], s.N), _g(grads[3 * p + 1], s.L), _g(grads[3 * p + 2], s.N)
+            fix = None
+            if ctx.clamps[p] is not None:   # constant-HP clamp branch: Woodbury, this plan
+                gH, fix = _clamp_rhs(s, plans[p], B, ctx.clamps[p], gH, gQ, gE,
+                                     torch.cuda.current_stream(dev).cuda_stream)
+            fixes.append(fix)
             gd = torch.empty(B, s.N, dtype=torch.float64, device=dev)
             grh, gke = torch.empty_like(gd), torch.empty_like(gd)
             gr = torch.empty(B, s.L, dtype=torch.float64, device=dev)
@@ -169,6 +174,9 @@ class ImplicitMultiSM100(torch.autograd.Function):
         _lib.check(plans[0].lib.wds_adjoint_multi(n, handles, batch, io,
                                                   ctypes.c_void_p(cur.cuda_stream)),
                    "wds_adjoint_multi")
+        for p in range(n):
+            if fixes[p] is not None:
+                _clamp_grh(fixes[p], keep[3 * p + 1], outs[p][0], outs[p][1])
         # [B, *] gradients; autograd sums them to a 1-D or single-row input's
         # shape (the batch sum of dgga/autodiff.py:1306-1308)
         res = []
