@@ -220,7 +220,7 @@ def run_reference(args, rank, world):
 
 # ------------------------------------------------------------------ secondary workloads
 def run_secondary(args):
-    """Mixed-size one-launch and extended-period workloads: one JSON line."""
+    """Mixed-size one-launch, extended-period and unrolled-K workloads: one JSON line."""
     import torch
     from wdsgpu_b200 import synth
     from wdsgpu_b200.solver import GGASolver
@@ -254,6 +254,39 @@ def run_secondary(args):
                            "782 jn/905 pipes/3 PRVs, 3000 jn/3600 pipes; instances per network %s; "
                            "lognormal(0.3) demands" % counts.tolist(),
                "instances": units, "launches_per_step": 2}
+    elif args.workload == "unrolled":
+        from wdsgpu_b200.autodiff import solve_unrolled
+        from wdsgpu_b200.net import PIPE, PRV
+        base = synth.config2_network()
+        f = base.as_fields()                     # the unrolled route takes no PRVs
+        lt = np.asarray(base.link_type).copy()
+        st = np.asarray(base.init_status).copy()
+        st[lt == PRV] = 1
+        lt[lt == PRV] = PIPE
+        f["link_type"], f["init_status"] = lt.astype(np.int8), st.astype(np.int8)
+        net = synth.Net(**f)
+        s = GGASolver(net, device=dev, dense_status_machine=True)
+        B, K = 1024, 14
+        d, rh = synth.config2_scenarios(net, B, seed=7)
+        d = torch.as_tensor(d, device=dev)
+        rh = torch.as_tensor(rh, device=dev)
+        sens = torch.as_tensor(synth.sensor_nodes(net, N_SENSORS), device=dev)
+
+        def step():
+            D = d.clone().requires_grad_(True)
+            out = solve_unrolled(s, D, rh, K=K)
+            (out["head_ft"][:, sens] ** 2).sum().backward()
+            return float(D.grad.abs().sum())
+
+        units = B
+        metric = "unrolled-K fwd+reverse scenarios/s (782 jn, K=14, B=1024)"
+        unit = "scenarios/s"
+        cfg = {"workload": "782-junction synthetic looped network with its 3 PRVs as open "
+                           "pipes (the unrolled route takes no control valves); B=1024 "
+                           "lognormal(0.2) demands; K=14 fixed GGA iterations recorded, then "
+                           "the reverse pass over them (one factor and one solve per "
+                           "iteration); grads w.r.t. demand of sum of squared heads at 30 "
+                           "sensors", "B": B, "K": K}
     else:
         from wdsgpu_b200.eps import eps_solve
         net0 = synth.config5_network()
@@ -316,7 +349,7 @@ def main():
     ap.add_argument("--impl", default="sm100", choices=("sm100", "reference"))
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=("config2", "mixed", "eps"))
+    ap.add_argument("--workload", default="config2", choices=("config2", "mixed", "eps", "unrolled"))
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
