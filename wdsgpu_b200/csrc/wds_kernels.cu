@@ -1005,12 +1005,18 @@ __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const
   gsync<NT>();
 }
 
-// Primal reduced Newton solve with ACTIVE-PRV Dirichlet / merged rows
-// (dgga/autodiff.py:965-1029): M_p differs from the factored matrix by 2p row
-// replacements, applied by Woodbury and two outer refinement steps against the
-// true M_p.  The Woodbury columns A^{-1} e_u come from one substitution each;
-// the outer refinement makes the result independent of their rounding.
-// rhs: V0 (kept), result in dH.
+// Primal reduced Newton solve with ACTIVE control valves (the system of
+// dgga/autodiff.py:965-1029): an ACTIVE valve fixes the head it holds
+// (dH_jc = -r_valve) and frees its flow, which enters the balance rows as the
+// column u = sgn (e_jc - e_jo) (sgn +1 for a PRV, jc = n2; -1 for a PSV,
+// jc = n1).  With dH_jc known, the unknowns are the other heads and the valve
+// flow in slot jc: M y = r', M = the factored A with column jc replaced by u
+// (the transpose of the adjoint's row-replaced matrix), r' = rhs - A_red[:,jc]
+// dH_jc.  Woodbury on the factor: A^{-1} u_a - e_jc (one solve per active
+// valve, right-hand side e_jc - e_jo), C_ab = X_b[jc_a], and two outer
+// refinement steps against the true M make the result independent of the
+// unrefined inner solves.  Output: dH (with dH_jc = -r_valve) and the valve
+// flow corrections dqv[p].  rhs: V0 (kept).
 template <int NT, class FT, class TB>
 __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
@@ -1022,91 +1028,100 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
     solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, 2);
     return;
   }
-  const int p = n.npcv, m = 2 * p;
-  double* C = s.small;            // m*m
-  double* y = s.small + m * m;    // m
-  double* actf = y + m;           // p
-  double* row1 = actf + p;        // p
+  const int p = n.npcv;
+  double* C = s.small;             // p*p
+  double* y = s.small + 4 * p * p; // p
+  double* actf = y + 2 * p;        // p
+  double* dqv = actf + p;          // p, output
   if (tid == 0)
     for (int i = 0; i < p; ++i) actf[i] = s.S[n.pcv_link[i]] == WDS_ACTIVE ? 1.0 : 0.0;
-  for (int q = tid; q < n.Nj; q += NT) rp[q] = rhs[q];
+  for (int q = tid; q < n.Nj; q += NT) sx[q] = 0.0;
   gsync<NT>();
-  if (tid == 0) {
-    // rp[jo] += rhs[jc] (ACTIVE), then rp[jc] = -r_prv (jc: the held head)
+  if (tid == 0)
     for (int i = 0; i < p; ++i)
-      if (actf[i] != 0.0) rp[n.pcv_jo[i]] += rhs[n.pcv_jc[i]];
-    for (int i = 0; i < p; ++i)
-      if (actf[i] != 0.0) rp[n.pcv_jc[i]] = -rprv[i];
+      if (actf[i] != 0.0) sx[n.pcv_jc[i]] = -rprv[i];
+  gsync<NT>();
+  // r' = rhs - A_red dH_fixed (A_red: the factored matrix without the valves' penalty)
+  for (int q = tid; q < n.Nj; q += NT) {
+    double acc = amul_node(n, T, s, q, sx);
+    for (int c = n.cb_ptr[q]; c < n.cb_ptr[q + 1]; ++c)
+      acc -= sx[q] * (s.S[n.pcv_link[n.cb_idx[c]]] == WDS_ACTIVE ? kCBIG : 0.0);
+    rp[q] = rhs[q] - acc;
   }
   gsync<NT>();
-  // The outer refinement below (two steps against the true M_p) contracts the
-  // error of this solve and of its own corrections by about kappa * u each, so
-  // these solves take no inner refinement; the fixed point is set by the FP64
-  // residual and does not depend on it.
+  // the outer refinement below contracts the error of these unrefined solves
   solve_refined<NT, FT>(n, T, s, rp, -1, dH, t, 0);
-  for (int c = 0; c < m; ++c) {
-    // columns of inactive valves meet y = 0 in the correction: zero, not solved
-    if (actf[c < p ? c : c - p] == 0.0) {
-      for (int q = tid; q < n.Nj; q += NT) cols[(size_t)c * n.Nj + q] = 0.0;
+  for (int c = 0; c < p; ++c) {  // X_c = A^{-1} sgn_c (e_jc - e_jo); zero for inactive valves
+    double* xc = cols + (size_t)c * n.Nj;
+    if (actf[c] == 0.0) {
+      for (int q = tid; q < n.Nj; q += NT) xc[q] = 0.0;
       gsync<NT>();
       continue;
     }
-    const int u = c < p ? n.pcv_jc[c] : n.pcv_jo[c - p];
-    solve_refined<NT, FT>(n, T, s, nullptr, u, cols + (size_t)c * n.Nj, t, 0);
-  }
-  if (tid == 0) {
-    // C = [R2 ; I2 - CBIG R2], rows of inactive valves -> identity
-    for (int a = 0; a < p; ++a)
-      for (int c = 0; c < m; ++c) {
-        const double r2 = cols[(size_t)c * n.Nj + n.pcv_jc[a]];
-        const double i2 = (c == a || c == a + p) ? 1.0 : 0.0;
-        C[a * m + c] = actf[a] != 0.0 ? r2 : (c == a ? 1.0 : 0.0);
-        C[(a + p) * m + c] = actf[a] != 0.0 ? i2 - kCBIG * r2 : (c == a + p ? 1.0 : 0.0);
-      }
-  }
-  gsync<NT>();
-  // x <- x - S y,  y = C^{-1} [ (x[jc]-rr[jc]) act ; (rr[jc] - CBIG x[jc]) act ]
-  auto wood = [&](double* x, const double* rr) {
+    for (int q = tid; q < n.Nj; q += NT) res[q] = 0.0;
+    gsync<NT>();
     if (tid == 0) {
-      double Cc[64];
-      for (int i = 0; i < m * m; ++i) Cc[i] = C[i];
-      for (int a = 0; a < p; ++a) {
-        const int jc = n.pcv_jc[a];
-        y[a] = (x[jc] - rr[jc]) * actf[a];
-        y[a + p] = (rr[jc] - kCBIG * x[jc]) * actf[a];
-      }
-      dense_solve(Cc, y, m);
+      res[n.pcv_jc[c]] = n.pcv_sgn[c];
+      res[n.pcv_jo[c]] = -n.pcv_sgn[c];
+    }
+    gsync<NT>();
+    solve_refined<NT, FT>(n, T, s, res, -1, xc, t, 0);
+  }
+  if (tid == 0)
+    for (int a0 = 0; a0 < p; ++a0)
+      for (int c = 0; c < p; ++c)
+        C[a0 * p + c] = actf[a0] != 0.0 ? cols[(size_t)c * n.Nj + n.pcv_jc[a0]]
+                                         : (a0 == c ? 1.0 : 0.0);
+  gsync<NT>();
+  // x <- x - sum_b z_b (X_b - e_jc_b),  z = C^{-1} (x[jc] act)
+  auto wood = [&](double* x) {
+    if (tid == 0) {
+      double Cc[16];
+      for (int i = 0; i < p * p; ++i) Cc[i] = C[i];
+      for (int a0 = 0; a0 < p; ++a0) y[a0] = x[n.pcv_jc[a0]] * actf[a0];
+      dense_solve(Cc, y, p);
     }
     gsync<NT>();
     for (int q = tid; q < n.Nj; q += NT) {
       double acc = 0.0;
-      for (int c = 0; c < m; ++c) acc += cols[(size_t)c * n.Nj + q] * y[c];
+      for (int c = 0; c < p; ++c) acc += cols[(size_t)c * n.Nj + q] * y[c];
       x[q] = x[q] - acc;
     }
     gsync<NT>();
+    if (tid == 0)
+      for (int c = 0; c < p; ++c) x[n.pcv_jc[c]] += y[c] * actf[c];
+    gsync<NT>();
   };
-  wood(dH, rp);
+  wood(dH);
   for (int it = 0; it < 2; ++it) {
-    for (int q = tid; q < n.Nj; q += NT) res[q] = amul_node(n, T, s, q, dH);
+    // res = r' - M y, M y = A y_z + sum_a u_a y_jc (y_z: y with the valve slots zero)
+    for (int q = tid; q < n.Nj; q += NT) sx[q] = dH[q];
     gsync<NT>();
     if (tid == 0)
       for (int i = 0; i < p; ++i)
-        row1[i] = res[n.pcv_jo[i]] + res[n.pcv_jc[i]] - kCBIG * dH[n.pcv_jc[i]];
+        if (actf[i] != 0.0) sx[n.pcv_jc[i]] = 0.0;
     gsync<NT>();
-    for (int q = tid; q < n.Nj; q += NT) res[q] = rp[q] - res[q];
+    for (int q = tid; q < n.Nj; q += NT) res[q] = rp[q] - amul_node(n, T, s, q, sx);
     gsync<NT>();
-    if (tid == 0) {
+    if (tid == 0)
       for (int i = 0; i < p; ++i)
-        if (actf[i] != 0.0) res[n.pcv_jo[i]] = rp[n.pcv_jo[i]] - row1[i];
-      for (int i = 0; i < p; ++i)
-        if (actf[i] != 0.0) res[n.pcv_jc[i]] = rp[n.pcv_jc[i]] - dH[n.pcv_jc[i]];
-    }
+        if (actf[i] != 0.0) {
+          const double v = n.pcv_sgn[i] * dH[n.pcv_jc[i]];
+          res[n.pcv_jc[i]] -= v;
+          res[n.pcv_jo[i]] += v;
+        }
     gsync<NT>();
     solve_refined<NT, FT>(n, T, s, res, -1, sx, t, 0);
-    wood(sx, res);
+    wood(sx);
     for (int q = tid; q < n.Nj; q += NT) dH[q] = dH[q] + sx[q];
     gsync<NT>();
   }
+  if (tid == 0)
+    for (int i = 0; i < p; ++i) {
+      dqv[i] = actf[i] != 0.0 ? dH[n.pcv_jc[i]] : 0.0;
+      if (actf[i] != 0.0) dH[n.pcv_jc[i]] = -rprv[i];
+    }
+  gsync<NT>();
 }
 
 __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) / 16 * 16; }
@@ -1490,11 +1505,8 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
-        if (i >= 0 && s.S[k] == WDS_ACTIVE) {  // the free valve flow, from the balance at jc
-          const int jc = n.pcv_jc[i];
-          const double abc = amul_node(n, T, s, jc, s.V1) - kCBIG * s.V1[jc] * 1.0;
-          dq = n.pcv_sgn[i] * (s.V0[jc] - abc);
-        }
+        if (i >= 0 && s.S[k] == WDS_ACTIVE)  // the free valve flow, solved in slot jc
+          dq = s.small[4 * n.npcv * n.npcv + 3 * n.npcv + i];
         s.q[k] = s.q[k] + dq;
       }
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
