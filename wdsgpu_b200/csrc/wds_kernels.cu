@@ -1014,18 +1014,19 @@ __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const
 // (the transpose of the adjoint's row-replaced matrix), r' = rhs - A_red[:,jc]
 // dH_jc.  Woodbury on the factor: A^{-1} u_a - e_jc (one solve per active
 // valve, right-hand side e_jc - e_jo), C_ab = X_b[jc_a], and two outer
-// refinement steps against the true M make the result independent of the
-// unrefined inner solves.  Output: dH (with dH_jc = -r_valve) and the valve
-// flow corrections dqv[p].  rhs: V0 (kept).
+// refinement steps against the true M (`outer`, two on the last polish step)
+// make the result independent of the unrefined inner solves.  Output: dH
+// (with dH_jc = -r_valve) and the valve flow corrections dqv[p].  rhs: V0
+// (kept).
 template <int NT, class FT, class TB>
 __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
-                             bool any_act) {
+                             bool any_act, int outer) {
   const double* rhs = s.V0;
   double* t = s.V2;
   const int tid = gtid<NT>();
-  if (!any_act) {  // two refinement steps, as the reference's polish solves
-    solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, 2);
+  if (!any_act) {  // `outer` refinement steps (two on the last polish step)
+    solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, outer);
     return;
   }
   const int p = n.npcv;
@@ -1093,7 +1094,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
     gsync<NT>();
   };
   wood(dH);
-  for (int it = 0; it < 2; ++it) {
+  for (int it = 0; it < outer; ++it) {
     // res = r' - M y, M y = A y_z + sum_a u_a y_jc (y_z: y with the valve slots zero)
     for (int q = tid; q < n.Nj; q += NT) sx[q] = dH[q];
     gsync<NT>();
@@ -1499,7 +1500,10 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
         s.V0[p] = (mm - bt) + emh * re;
       }
       gsync<NT>();
-      primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act);
+      // a Newton step corrects the rounding of the step before it: only the
+      // last polish step's solve sets the final state, so it alone refines
+      primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act,
+                           step == a.polish - 1 ? 2 : 0);
       // dq, de, state update
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
