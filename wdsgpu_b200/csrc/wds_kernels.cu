@@ -1222,31 +1222,53 @@ __device__ bool build_emitters(const DevNet& n, const Sh& s, const double* val, 
   return !gsync_or<NT>(over);
 }
 
-// ---------------------------------------------------------------- forward kernel
-// Forward of one CTA (block `blk` of the plan, `groups` scenario groups of NT
-// threads; groups beyond it, in a CTA with more threads, stay idle).
-template <int NT, class TB, class FT>
-__device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, const FwdArgs& a,
-                                             int state_bytes, int blk, int groups) {
+// ---------------------------------------------------------------- CTA scenario rounds
+// The CTAs of a launch are persistent: CTA `blk` of the `nblk` that run a plan
+// holds `groups` scenario groups of NT threads (groups beyond it, in a CTA
+// with more threads, stay idle), and group g takes scenario
+// b = (r * groups + g) * nblk + blk in rounds r = 0, 1, ... while b < B.  The
+// first nblk scenarios of a round go to group 0 of every CTA, so a partial
+// last round runs one group per SM instead of filling a few CTAs, and a group
+// with fewer co-resident groups runs faster (the kernels are latency-bound).
+// The schedule tables are staged into shared memory once per CTA; a group's
+// scenario state is its own slice of shared memory (global memory, per
+// scenario, on the large-network layout), reused from round to round behind a
+// group barrier.  `one(T, s, b)` solves scenario b.
+template <int NT, class TB, class One>
+__device__ __forceinline__ void cta_rounds(const DevNet& n, const DevWork& w, int B,
+                                           int state_bytes, int blk, int nblk, int groups,
+                                           One&& one) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / NT;
-  const int b = blk * groups + g;
   TB T;
-  Sh s;
   if constexpr (TB::kWide) {
-    // large network: tables and scenario state stay in global memory
-    if (g >= groups || b >= a.B) return;
     T = tab_view<TB>(n, (const unsigned char*)n.stab);
-    s = carve(n, w.state + (size_t)b * state_bytes);
   } else {
-    // stage the schedule tables once per CTA
     for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
       ((uint4*)smem_raw)[i] = n.stab[i];
     __syncthreads();
     T = tab_view<TB>(n, smem_raw);
-    if (g >= groups || b >= a.B) return;  // a whole group; groups use their own barriers
-    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
   }
+  if (g >= groups) return;  // a whole group; groups use their own barriers
+  for (int r = 0;; ++r) {
+    const long long bl = ((long long)r * groups + g) * nblk + blk;
+    if (bl >= B) return;  // uniform per group
+    const int b = (int)bl;
+    if (r > 0) gsync<NT>();  // the previous scenario's last reads of the group state
+    Sh s;
+    if constexpr (TB::kWide)
+      s = carve(n, w.state + (size_t)b * state_bytes);
+    else
+      s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
+    one(T, s, b);
+  }
+}
+
+// ---------------------------------------------------------------- forward kernel
+// Forward of scenario b by one scenario group.
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, const FwdArgs& a,
+                                            const TB& T, Sh s, int b) {
   s.q = w.lk + (size_t)b * 2 * n.L;
   s.Y = s.q + n.L;
   s.Mg = w.M + (size_t)b * n.nT * n.nT;
@@ -1597,30 +1619,21 @@ __device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, 
   }
 }
 
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void forward_body(const DevNet& n, const DevWork& w, const FwdArgs& a,
+                                             int state_bytes, int blk, int nblk, int groups) {
+  cta_rounds<NT, TB>(n, w, a.B, state_bytes, blk, nblk, groups, [&](const TB& T, Sh s, int b) {
+    forward_one<NT, TB, FT>(n, w, a, T, s, b);
+  });
+}
+
 // ---------------------------------------------------------------- adjoint kernel
 // Node adjoint with constraint rows (autodiff.py:1107-1154) and the
 // theta contraction (autodiff.py:1246-1312).
-// Adjoint of one CTA (as forward_body).
+// Adjoint of right-hand side b by one scenario group.
 template <int NT, class TB, class FT>
-__device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, const AdjArgs& a,
-                                             int state_bytes, int blk, int groups) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int g = threadIdx.x / NT;
-  const int b = blk * groups + g;
-  TB T;
-  Sh s;
-  if constexpr (TB::kWide) {
-    if (g >= groups || b >= a.B) return;
-    T = tab_view<TB>(n, (const unsigned char*)n.stab);
-    s = carve(n, w.state + (size_t)b * state_bytes);
-  } else {
-    for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
-      ((uint4*)smem_raw)[i] = n.stab[i];
-    __syncthreads();
-    T = tab_view<TB>(n, smem_raw);
-    if (g >= groups || b >= a.B) return;
-    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
-  }
+__device__ __forceinline__ void adjoint_one(const DevNet& n, const DevWork& w, const AdjArgs& a,
+                                            const TB& T, Sh s, int b) {
   // kept state of scenario bf (several right-hand sides per scenario read the
   // same factor); right-hand sides, results and scratch are per b
   const int bf = (a.v0 + b) / (a.rhs_per > 1 ? a.rhs_per : 1);
@@ -1793,6 +1806,14 @@ __device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, 
   }
 }
 
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void adjoint_body(const DevNet& n, const DevWork& w, const AdjArgs& a,
+                                             int state_bytes, int blk, int nblk, int groups) {
+  cta_rounds<NT, TB>(n, w, a.B, state_bytes, blk, nblk, groups, [&](const TB& T, Sh s, int b) {
+    adjoint_one<NT, TB, FT>(n, w, a, T, s, b);
+  });
+}
+
 // ---------------------------------------------------------------- unrolled-K reverse
 // dP/dq, dY/dq, dP/dr, dY/dr of one link on the branch its coefficients took
 // (the formulas of solve_unrolled, dgga/autodiff.py:1495-1591, differentiated
@@ -1916,25 +1937,8 @@ __device__ __forceinline__ void emitter_dcoef(const DevNet& n, double e, double 
 // lists (no atomics).  Scratch per scenario: qb [L], a link temporary [L],
 // eb [Nj], Fb [Nj].
 template <int NT, class TB, class FT>
-__device__ __forceinline__ void unrolled_body(const DevNet& n, const DevWork& w, const UnrollArgs& u,
-                                              int state_bytes, int blk, int groups) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int g = threadIdx.x / NT;
-  const int b = blk * groups + g;
-  TB T;
-  Sh s;
-  if constexpr (TB::kWide) {
-    if (g >= groups || b >= u.B) return;
-    T = tab_view<TB>(n, (const unsigned char*)n.stab);
-    s = carve(n, w.state + (size_t)b * state_bytes);
-  } else {
-    for (int i = threadIdx.x; i < n.stab_bytes / 16; i += blockDim.x)
-      ((uint4*)smem_raw)[i] = n.stab[i];
-    __syncthreads();
-    T = tab_view<TB>(n, smem_raw);
-    if (g >= groups || b >= u.B) return;
-    s = carve(n, smem_raw + n.stab_bytes + (size_t)g * state_bytes);
-  }
+__device__ __forceinline__ void unrolled_one(const DevNet& n, const DevWork& w, const UnrollArgs& u,
+                                             const TB& T, Sh s, int b) {
   const int tid = gtid<NT>();
   s.q = w.lk + (size_t)b * 2 * n.L;
   s.Y = s.q + n.L;
@@ -2077,22 +2081,30 @@ __device__ __forceinline__ void unrolled_body(const DevNet& n, const DevWork& w,
   }
 }
 
+template <int NT, class TB, class FT>
+__device__ __forceinline__ void unrolled_body(const DevNet& n, const DevWork& w, const UnrollArgs& u,
+                                              int state_bytes, int blk, int nblk, int groups) {
+  cta_rounds<NT, TB>(n, w, u.B, state_bytes, blk, nblk, groups, [&](const TB& T, Sh s, int b) {
+    unrolled_one<NT, TB, FT>(n, w, u, T, s, b);
+  });
+}
+
 template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_unrolled(DevNet n, DevWork w, UnrollArgs u,
                                                          int state_bytes) {
-  unrolled_body<NT, TB, FT>(n, w, u, state_bytes, blockIdx.x, GR);
+  unrolled_body<NT, TB, FT>(n, w, u, state_bytes, blockIdx.x, gridDim.x, GR);
 }
 
 template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_forward(DevNet n, DevWork w, FwdArgs a,
                                                         int state_bytes) {
-  forward_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, GR);
+  forward_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, gridDim.x, GR);
 }
 
 template <int NT, int GR, class TB, class FT>
 __global__ void __launch_bounds__(NT * GR, 1) k_adjoint(DevNet n, DevWork w, AdjArgs a,
                                                         int state_bytes) {
-  adjoint_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, GR);
+  adjoint_body<NT, TB, FT>(n, w, a, state_bytes, blockIdx.x, gridDim.x, GR);
 }
 
 // Several plans (networks of different sizes) in one launch: CTAs
@@ -2105,9 +2117,11 @@ __global__ void __launch_bounds__(768, 1) k_forward_multi(const __grid_constant_
   while (p + 1 < jobs.n && (int)blockIdx.x >= jobs.j[p + 1].cta0) ++p;
   const FwdJob& J = jobs.j[p];
   if (J.n.wide)
-    forward_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+    forward_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0,
+                                (J.a.B + J.groups - 1) / J.groups, J.groups);
   else
-    forward_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+    forward_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0,
+                                (J.a.B + J.groups - 1) / J.groups, J.groups);
 }
 
 template <class FT>
@@ -2116,14 +2130,31 @@ __global__ void __launch_bounds__(768, 1) k_adjoint_multi(const __grid_constant_
   while (p + 1 < jobs.n && (int)blockIdx.x >= jobs.j[p + 1].cta0) ++p;
   const AdjJob& J = jobs.j[p];
   if (J.n.wide)
-    adjoint_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+    adjoint_body<256, LTab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0,
+                                (J.a.B + J.groups - 1) / J.groups, J.groups);
   else
-    adjoint_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0, J.groups);
+    adjoint_body<256, STab, FT>(J.n, J.w, J.a, J.state_bytes, blockIdx.x - J.cta0,
+                                (J.a.B + J.groups - 1) / J.groups, J.groups);
 }
 
 }  // namespace
 
 size_t state_smem_bytes(const DevNet& n) { return smem_bytes(n); }
+
+// CTAs of a persistent launch of B scenarios: one per scenario, at most as
+// many as the device keeps resident at once (SMs x CTAs per SM for the
+// kernel's threads and shared memory); the CTAs take the scenarios in rounds.
+template <class K>
+static cudaError_t persistent_grid(K kern, int threads, size_t smem, int B, int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (ce == cudaSuccess)
+    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (ce == cudaSuccess && per_sm < 1) ce = cudaErrorInvalidConfiguration;
+  *grid = std::max(1, std::min(B, sms * per_sm));
+  return ce;
+}
 
 template <class Jobs>
 static size_t multi_smem(const Jobs& jobs) {
@@ -2218,9 +2249,12 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int grou
     *err = std::string("wds_forward: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
-  const int grid = (a.B + groups - 1) / groups;
-  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
-  ce = cudaGetLastError();
+  int grid = 1;
+  ce = persistent_grid(kern, 256 * groups, smem, a.B, &grid);
+  if (ce == cudaSuccess) {
+    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
+    ce = cudaGetLastError();
+  }
   if (ce != cudaSuccess) {
     *err = std::string("wds_forward launch: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
@@ -2228,8 +2262,9 @@ int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int grou
   return WDS_OK;
 }
 
-int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int groups,
+int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int plan_groups,
                     void* stream, std::string* err) {
+  const int groups = std::min(plan_groups, 3);  // the reverse pass runs at most 3 groups per CTA
   const int st = (int)smem_bytes(n);
   const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
   void (*kern)(DevNet, DevWork, UnrollArgs, int) =
@@ -2244,9 +2279,12 @@ int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int 
     *err = std::string("wds_unrolled_adjoint: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
-  const int grid = (u.B + groups - 1) / groups;
-  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, u, st);
-  ce = cudaGetLastError();
+  int grid = 1;
+  ce = persistent_grid(kern, 256 * groups, smem, u.B, &grid);
+  if (ce == cudaSuccess) {
+    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, u, st);
+    ce = cudaGetLastError();
+  }
   if (ce != cudaSuccess) {
     *err = std::string("wds_unrolled_adjoint launch: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
@@ -2276,9 +2314,12 @@ int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int grou
     *err = std::string("wds_adjoint: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
   }
-  const int grid = (a.B + groups - 1) / groups;
-  kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
-  ce = cudaGetLastError();
+  int grid = 1;
+  ce = persistent_grid(kern, 256 * groups, smem, a.B, &grid);
+  if (ce == cudaSuccess) {
+    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
+    ce = cudaGetLastError();
+  }
   if (ce != cudaSuccess) {
     *err = std::string("wds_adjoint launch: ") + cudaGetErrorString(ce);
     return WDS_E_CUDA;
