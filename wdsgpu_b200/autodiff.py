@@ -195,9 +195,9 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         o = s.run(d, rh, ke_t, r_t, B, int(max_iter), float(accuracy), sm, int(polish_steps),
                   pumps=pumps)
         info = o["info"]
-        from .solver import _check_emitter_cap
-        _check_emitter_cap(s, info)
-        if bool((info != 0).any()):
+        if bool((info != 0).any()):   # one host sync when every scenario converged
+            from .solver import _check_emitter_cap
+            _check_emitter_cap(s, info)
             bad = torch.nonzero(info != 0).flatten().tolist()
             np_ = torch.nonzero(info & _lib.INFO_NOT_PD).flatten().tolist()
             if np_:

@@ -218,6 +218,7 @@ class GGASolver:
         is_junc = nt == 0
         self.junc_nodes = np.flatnonzero(is_junc)
         self.fixed_nodes = np.flatnonzero(~is_junc)
+        self._fixed_dev = None
         self.Nj = int(is_junc.sum())
         self.hexp = 1.852 if self.headloss_form == "H-W" else 2.0
         self.qexp = float(meta["qexp"])
@@ -491,7 +492,9 @@ class GGASolver:
         rh = rh.contiguous()
         ke = ke.contiguous()
         r = r.contiguous()
-        if torch.isnan(rh[:, torch.as_tensor(self.fixed_nodes, device=self.device)]).any():
+        if self._fixed_dev is None:   # device copy of the reservoir/tank node index, once
+            self._fixed_dev = torch.as_tensor(self.fixed_nodes, device=self.device)
+        if torch.isnan(rh.index_select(1, self._fixed_dev)).any():
             raise ValueError("res_head_ft is nan at a reservoir/tank node")
         return d, rh, ke, r, B, single
 
