@@ -5,8 +5,8 @@
  * the reference's batched GGA route (dgga/solver.py:2922-3179,
  * `_cudss_forward` :2630, `_cudss_factor` :2683, `_cudss_adjoint` :2653) and
  * the GPU implicit adjoint (dgga/autodiff.py:1157-1312, `_kf_prepare` /
- * `_kf_solve` :898-925).  A binding from the reference would call these four
- * entry points through ctypes with plain pointers.
+ * `_kf_solve` :898-925).  A binding from the reference calls these entry
+ * points through ctypes with plain pointers.
  *
  * Units are EPANET internal units (ft, cfs).  All array arguments of
  * wds_forward / wds_adjoint are DEVICE pointers owned by the caller; the plan
@@ -235,6 +235,16 @@ int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K, const double* 
  * n_pcv, nnz_A_lower, threads]. */
 int wds_plan_stats(const WdsPlan* plan, int64_t* out8);
 
+/* Generation of the plan's kept state: a counter that changes with every
+ * call that rewrites the plan's workspace (wds_forward, wds_forward_multi,
+ * wds_unrolled_adjoint).  A caller that differentiates later records it
+ * after its implicit forward and checks it before wds_adjoint, so that a
+ * forward run in between (which replaces the terminal factor) is an error
+ * and never a silent gradient of the other call.  The reference keeps one
+ * factor per autograd context (`ctx.kf`, dgga/autodiff.py:1203-1243); here a
+ * caller with several pending backwards gives each its own plan. */
+int wds_state_generation(const WdsPlan* plan, int64_t* gen);
+
 /* Host copy of the symbolic structure: perm [Nj], colptr [Nj+1],
  * rowidx [nnz_L], parent [Nj], level [Nj] (any pointer may be NULL). */
 int wds_plan_symbolic(const WdsPlan* plan, int32_t* perm, int32_t* colptr,
@@ -295,15 +305,20 @@ int wds_adjoint_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batc
 #define WDS_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* Forward without allocation (no counterpart in the reference, which always
- * allocates through torch).  Same arguments and results as wds_forward, but
- * the per-scenario workspace lives in one fixed WDS_NOALLOC_SCRATCH_BYTES
- * device array held by every GPU that loads the library, so the call never
- * calls cudaMalloc: for solve loops that must not allocate, or that run
- * inside stream capture.  A batch whose workspace exceeds the array is
- * rejected with WDS_E_ARG.  The first call on a device looks up the array's
- * device address and should come before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race and must be serialised.  The call
- * does not prepare wds_adjoint. */
+ * allocates through torch).  For callers that cannot call cudaMalloc when
+ * they solve: a control loop that allocates everything at start-up because
+ * an allocation can stall it, or a host whose device memory belongs to
+ * another allocator.  Same arguments and results as wds_forward, but the
+ * per-scenario workspace lives in one fixed WDS_NOALLOC_SCRATCH_BYTES device
+ * array held by every GPU that loads the library until the process exits,
+ * so the call never calls cudaMalloc or cudaFree.  A batch whose workspace
+ * exceeds the array (about 400 scenarios of a 782-junction network) is
+ * rejected with WDS_E_ARG.  The first call on a device loads the library's
+ * device code there, which creates the array; make that first call before
+ * any stream capture.  Calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  The call does not
+ * prepare wds_adjoint. */
 int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const WdsForwardOpts* opts,
                         const double* demand, const double* fixed_head,
                         const double* ke, const double* r,

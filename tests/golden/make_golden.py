@@ -1,7 +1,8 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Runs only in a container where the reference package (`dgga`) sits at
-REFERENCE_ROOT (default /root/reference); the fixtures it writes are small
+Runs only where the reference package (`dgga`) is importable from the
+directory named by the REFERENCE_ROOT environment variable (required); the
+fixtures it writes are small
 .npz files that travel with the tests.  The reference imports `wntr` at module
 top for its INP parser only; that package is absent offline, so a stub with
 the imported names is placed in sys.modules (the parser is never called: the
@@ -15,7 +16,7 @@ and the reference outputs of
   * for small cases, implicit_solve(..., adjoint="cpu") on mode="epanet"
     (the EPANET-replica path with the scipy splu adjoint).
 
-Usage:  python tests/golden/make_golden.py        (steady cases)
+Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
         python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
         python tests/golden/make_golden.py sens   (sensitivity-matrix pin, sens_ref.npz)
         python tests/golden/make_golden.py pumps  (pump-parameter gradient pins, pump_ref.npz
@@ -33,7 +34,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT")
 
 
 def _install_wntr_stub():
@@ -53,6 +54,8 @@ def _install_wntr_stub():
 
 
 def _load_reference():
+    if not REFERENCE_ROOT:
+        raise SystemExit("set REFERENCE_ROOT to the directory that holds the reference's dgga")
     _install_wntr_stub()
     sys.path.insert(0, REFERENCE_ROOT)
     import dgga.autodiff

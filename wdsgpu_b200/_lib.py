@@ -24,7 +24,7 @@ E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
            -4: "unsupported network", -5: "no forward state"}
 
 EXPORTS = ("wds_plan", "wds_forward", "wds_adjoint", "wds_plan_stats",
-           "wds_plan_symbolic", "wds_free", "wds_last_error", "wds_forward_noalloc",
+           "wds_plan_symbolic", "wds_state_generation", "wds_free", "wds_last_error", "wds_forward_noalloc",
            "wds_forward_multi", "wds_adjoint_multi", "wds_adjoint_rhs", "wds_adjoint_pumps",
            "wds_unrolled_adjoint")
 MULTI_MAX = 8
@@ -121,6 +121,8 @@ def load():
     lib.wds_plan_stats.restype = ctypes.c_int
     lib.wds_plan_symbolic.argtypes = [vp] + [c_int32_p] * 5
     lib.wds_plan_symbolic.restype = ctypes.c_int
+    lib.wds_state_generation.argtypes = [vp, c_int64_p]
+    lib.wds_state_generation.restype = ctypes.c_int
     lib.wds_free.argtypes = [vp]
     lib.wds_free.restype = ctypes.c_int
     lib.wds_last_error.argtypes = []

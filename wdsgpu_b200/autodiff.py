@@ -33,7 +33,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .solver import CBIG, GGASolver, _not_pd_hint
+from .solver import CBIG, GGASolver, _Hold, _not_pd_hint
 
 __all__ = ["implicit_solve", "ImplicitGGASolveSM100", "solve_unrolled", "UnrolledSM100",
            "unrolled_grad_health", "hw_resistance", "dr_dC"]
@@ -212,6 +212,7 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         ctx.pumps = pumps      # keeps the rows alive with the kept state
         ctx.th = tuple(None if x is None else (x.dim(), x.device) for x in th_in)
         ctx.plan = o["plan"]
+        ctx.hold = _Hold(o["plan"])   # later forwards take another plan until the backward
         ctx.B = B
         ctx.dims = dims
         ctx.devs = devs
@@ -244,6 +245,7 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         gke = torch.empty_like(gd)
         gr = torch.empty(B, L, dtype=torch.float64, device=dev)
         p = ctx.plan
+        ctx.hold.check("implicit_solve backward")
         cur = torch.cuda.current_stream(dev)
         ev = s._event_pair(cur, "adjoint")
         fix = None
@@ -262,6 +264,7 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
                 p.handle, B, gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(),
                 grh.data_ptr(), gke.data_ptr(), gr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
                 "wds_adjoint")
+        ctx.hold.release()   # stream order keeps the adjoint ahead of a later forward
         if fix is not None:
             _clamp_grh(fix, gQ, gd, grh)
         if ev is not None:

@@ -1,4 +1,8 @@
-// Fused batched GGA forward and reduced implicit adjoint for sm_100a.
+// Device code of the fused batched GGA forward and reduced implicit adjoint
+// for sm_100a.  Included by the kernel-instance sources (wds_k_*.cu), each of
+// which instantiates one kernel kind in one factor precision, so that the
+// instances compile in parallel; the launchers (wds_launch.cu) reach them
+// through the kernel selectors at the end of this file.
 //
 // A CTA holds `GR` independent scenario groups of 256 threads.  Each group owns
 // one scenario at a time: its link flows and coefficients, the LDL^T factor of
@@ -24,6 +28,7 @@
 // Implicit mode then runs the reduced Newton polish with Woodbury row
 // replacement for ACTIVE PRVs (dgga/autodiff.py:965-1104) and stores the
 // terminal factor and coefficients for the adjoint kernel.
+#pragma once
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -2139,192 +2144,18 @@ __global__ void __launch_bounds__(768, 1) k_adjoint_multi(const __grid_constant_
 
 }  // namespace
 
-size_t state_smem_bytes(const DevNet& n) { return smem_bytes(n); }
-
-// CTAs of a persistent launch of B scenarios: one per scenario, at most as
-// many as the device keeps resident at once (SMs x CTAs per SM for the
-// kernel's threads and shared memory); the CTAs take the scenarios in rounds.
-template <class K>
-static cudaError_t persistent_grid(K kern, int threads, size_t smem, int B, int* grid) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t ce = cudaGetDevice(&dev);
-  if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (ce == cudaSuccess)
-    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-  if (ce == cudaSuccess && per_sm < 1) ce = cudaErrorInvalidConfiguration;
-  *grid = std::max(1, std::min(B, sms * per_sm));
-  return ce;
-}
-
-template <class Jobs>
-static size_t multi_smem(const Jobs& jobs) {
-  size_t smem = 0;
-  for (int p = 0; p < jobs.n; ++p) {
-    const auto& J = jobs.j[p];
-    if (!J.n.wide)
-      smem = std::max(smem, (size_t)J.n.stab_bytes + (size_t)J.groups * (size_t)J.state_bytes);
-  }
-  return smem;
-}
-
-int launch_forward_multi(FwdJobs& jobs, void* stream, std::string* err) {
-  int ctas = 0;
-  bool fp32 = false;
-  for (int p = 0; p < jobs.n; ++p) {
-    FwdJob& J = jobs.j[p];
-    if (J.n.npcv > 4) {
-      *err = "wds_forward_multi: more than 4 status-machine PRVs is not supported by this build";
-      return WDS_E_UNSUPPORTED;
-    }
-    if (p > 0 && (J.n.fp32 != 0) != fp32) {
-      *err = "wds_forward_multi: the plans mix FP32 and FP64 factors";
-      return WDS_E_ARG;
-    }
-    fp32 = J.n.fp32 != 0;
-    J.state_bytes = (int)smem_bytes(J.n);
-    J.cta0 = ctas;
-    ctas += (J.a.B + J.groups - 1) / J.groups;
-  }
-  const size_t smem = multi_smem(jobs);
-  void (*kern)(FwdJobs) = fp32 ? k_forward_multi<float> : k_forward_multi<double>;
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (ce == cudaSuccess && ctas > 0) {
-    kern<<<ctas, 768, smem, (cudaStream_t)stream>>>(jobs);
-    ce = cudaGetLastError();
-  }
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_forward_multi: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  return WDS_OK;
-}
-
-int launch_adjoint_multi(AdjJobs& jobs, void* stream, std::string* err) {
-  int ctas = 0;
-  bool fp32 = false;
-  for (int p = 0; p < jobs.n; ++p) {
-    AdjJob& J = jobs.j[p];
-    if (p > 0 && (J.n.fp32 != 0) != fp32) {
-      *err = "wds_adjoint_multi: the plans mix FP32 and FP64 factors";
-      return WDS_E_ARG;
-    }
-    fp32 = J.n.fp32 != 0;
-    J.state_bytes = (int)smem_bytes(J.n);
-    J.cta0 = ctas;
-    ctas += (J.a.B + J.groups - 1) / J.groups;
-  }
-  const size_t smem = multi_smem(jobs);
-  void (*kern)(AdjJobs) = fp32 ? k_adjoint_multi<float> : k_adjoint_multi<double>;
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (ce == cudaSuccess && ctas > 0) {
-    kern<<<ctas, 768, smem, (cudaStream_t)stream>>>(jobs);
-    ce = cudaGetLastError();
-  }
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_adjoint_multi: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  return WDS_OK;
-}
-
-int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
-                   void* stream, std::string* err) {
-  if (n.npcv > 4) {
-    *err = "wds_forward: more than 4 status-machine PRVs is not supported by this build";
-    return WDS_E_UNSUPPORTED;
-  }
-  const int st = (int)smem_bytes(n);
-  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
-  void (*kern)(DevNet, DevWork, FwdArgs, int) =
-      n.fp32 ? (n.wide ? k_forward<256, 1, LTab, float>
-                : groups == 1 ? k_forward<256, 1, STab, float>
-                : groups == 2 ? k_forward<256, 2, STab, float>
-                : groups == 3 ? k_forward<256, 3, STab, float> : k_forward<256, 4, STab, float>)
-             : (n.wide ? k_forward<256, 1, LTab, double>
-                : groups == 1 ? k_forward<256, 1, STab, double>
-                : groups == 2 ? k_forward<256, 2, STab, double>
-                : groups == 3 ? k_forward<256, 3, STab, double> : k_forward<256, 4, STab, double>);
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_forward: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  int grid = 1;
-  ce = persistent_grid(kern, 256 * groups, smem, a.B, &grid);
-  if (ce == cudaSuccess) {
-    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
-    ce = cudaGetLastError();
-  }
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_forward launch: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  return WDS_OK;
-}
-
-int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int plan_groups,
-                    void* stream, std::string* err) {
-  const int groups = std::min(plan_groups, 3);  // the reverse pass runs at most 3 groups per CTA
-  const int st = (int)smem_bytes(n);
-  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
-  void (*kern)(DevNet, DevWork, UnrollArgs, int) =
-      n.fp32 ? (n.wide ? k_unrolled<256, 1, LTab, float>
-                : groups == 1 ? k_unrolled<256, 1, STab, float>
-                : groups == 2 ? k_unrolled<256, 2, STab, float> : k_unrolled<256, 3, STab, float>)
-             : (n.wide ? k_unrolled<256, 1, LTab, double>
-                : groups == 1 ? k_unrolled<256, 1, STab, double>
-                : groups == 2 ? k_unrolled<256, 2, STab, double> : k_unrolled<256, 3, STab, double>);
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_unrolled_adjoint: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  int grid = 1;
-  ce = persistent_grid(kern, 256 * groups, smem, u.B, &grid);
-  if (ce == cudaSuccess) {
-    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, u, st);
-    ce = cudaGetLastError();
-  }
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_unrolled_adjoint launch: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  return WDS_OK;
-}
-
-int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int groups,
-                   void* stream, std::string* err) {
-  if (n.npcv > 4) {
-    *err = "wds_adjoint: more than 4 status-machine PRVs is not supported by this build";
-    return WDS_E_UNSUPPORTED;
-  }
-  const int st = (int)smem_bytes(n);
-  const size_t smem = n.wide ? 0 : (size_t)n.stab_bytes + (size_t)groups * st;
-  void (*kern)(DevNet, DevWork, AdjArgs, int) =
-      n.fp32 ? (n.wide ? k_adjoint<256, 1, LTab, float>
-                : groups == 1 ? k_adjoint<256, 1, STab, float>
-                : groups == 2 ? k_adjoint<256, 2, STab, float>
-                : groups == 3 ? k_adjoint<256, 3, STab, float> : k_adjoint<256, 4, STab, float>)
-             : (n.wide ? k_adjoint<256, 1, LTab, double>
-                : groups == 1 ? k_adjoint<256, 1, STab, double>
-                : groups == 2 ? k_adjoint<256, 2, STab, double>
-                : groups == 3 ? k_adjoint<256, 3, STab, double> : k_adjoint<256, 4, STab, double>);
-  cudaError_t ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_adjoint: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  int grid = 1;
-  ce = persistent_grid(kern, 256 * groups, smem, a.B, &grid);
-  if (ce == cudaSuccess) {
-    kern<<<grid, 256 * groups, smem, (cudaStream_t)stream>>>(n, w, a, st);
-    ce = cudaGetLastError();
-  }
-  if (ce != cudaSuccess) {
-    *err = std::string("wds_adjoint launch: ") + cudaGetErrorString(ce);
-    return WDS_E_CUDA;
-  }
-  return WDS_OK;
-}
+// Kernel selectors, one definition per instance source and factor precision
+// (declared in wds_internal.h): the host stub of the kernel for the plan's
+// layout and scenario groups per CTA.
+#ifndef WDS_FP32
+#define WDS_FP32 0
+#endif
+#if WDS_FP32
+using KFT = float;
+#define WDS_KSEL(name) name##_f32
+#else
+using KFT = double;
+#define WDS_KSEL(name) name##_f64
+#endif
 
 }  // namespace wds

@@ -1,5 +1,5 @@
 // Internal layout shared by the host planner (wds_plan.cu) and the kernels
-// (wds_kernels.cu).  Not part of the public ABI.
+// (wds_device.cuh, instantiated by wds_k_*.cu).  Not part of the public ABI.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -256,5 +256,19 @@ struct AdjJobs {
 };
 int launch_forward_multi(FwdJobs& jobs, void* stream, std::string* err);
 int launch_adjoint_multi(AdjJobs& jobs, void* stream, std::string* err);
+
+// Kernel instances (wds_k_*.cu, one source per kernel kind compiled once per
+// factor precision): the host stub for a layout (wide: large network, one
+// group) and a count of scenario groups per CTA.
+const void* forward_kernel_f64(int wide, int groups);
+const void* forward_kernel_f32(int wide, int groups);
+const void* adjoint_kernel_f64(int wide, int groups);
+const void* adjoint_kernel_f32(int wide, int groups);
+const void* unrolled_kernel_f64(int wide, int groups);
+const void* unrolled_kernel_f32(int wide, int groups);
+const void* forward_multi_kernel_f64();
+const void* forward_multi_kernel_f32();
+const void* adjoint_multi_kernel_f64();
+const void* adjoint_multi_kernel_f32();
 
 }  // namespace wds

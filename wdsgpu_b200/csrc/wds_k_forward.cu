@@ -1,0 +1,14 @@
+// k_forward instances of one factor precision (WDS_FP32 = 0: FP64, 1: FP32).
+#include "wds_device.cuh"
+
+namespace wds {
+const void* WDS_KSEL(forward_kernel)(int wide, int groups) {
+  if (wide) return (const void*)k_forward<256, 1, LTab, KFT>;
+  switch (groups) {
+    case 1: return (const void*)k_forward<256, 1, STab, KFT>;
+    case 2: return (const void*)k_forward<256, 2, STab, KFT>;
+    case 3: return (const void*)k_forward<256, 3, STab, KFT>;
+    default: return (const void*)k_forward<256, 4, STab, KFT>;
+  }
+}
+}  // namespace wds

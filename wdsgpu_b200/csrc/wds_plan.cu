@@ -16,7 +16,6 @@
 #include <cmath>
 #include <cstring>
 #include <map>
-#include <mutex>
 #include <set>
 #include <string>
 #include <vector>
@@ -80,6 +79,43 @@ struct Blob {
   }
 };
 
+// Byte offsets of the per-scenario workspace of `B` scenarios (terminal
+// factor and coefficients kept for the adjoint, scratch vectors, link flows,
+// top-block inverses, large-network state, pump derivatives), each array
+// 256-byte aligned.  One function for the plan's own workspace and for the
+// fixed array of wds_forward_noalloc, so the two layouts cannot drift apart.
+struct WorkOff {
+  size_t W, P, dr, emh, hge, dke, act, scr, valid, lk, M, state, pump, bytes;
+};
+
+WorkOff work_layout(const wds::DevNet& d, int nscr, size_t B, size_t state_bytes) {
+  WorkOff o{};
+  size_t bytes = 0;
+  auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
+  const size_t pc = (size_t)std::max(d.npcv, 1);
+  o.W = take(B * d.nnzL * 8); o.P = take(B * d.L * 8); o.dr = take(B * d.L * 8);
+  o.emh = take(B * d.Nj * 8); o.hge = take(B * d.Nj * 8); o.dke = take(B * d.Nj * 8);
+  o.act = take(B * pc); o.scr = take(B * (size_t)nscr * d.Nj * 8); o.valid = take(B * 4);
+  o.lk = take(B * 2 * d.L * 8); o.M = take(B * (size_t)std::max(d.nT * d.nT, 1) * 8);
+  o.state = take(d.wide ? B * state_bytes : 0); o.pump = take(B * 3 * (size_t)d.npump * 8);
+  o.bytes = bytes;
+  return o;
+}
+
+// The workspace arrays at `base` laid out by work_layout.
+wds::DevWork work_at(unsigned char* base, const WorkOff& o, const wds::DevNet& d, int nscr) {
+  wds::DevWork w{};
+  w.W = (double*)(base + o.W); w.P = (double*)(base + o.P); w.dr = (double*)(base + o.dr);
+  w.emh = (double*)(base + o.emh); w.hge = (double*)(base + o.hge);
+  w.dke = (double*)(base + o.dke); w.act = (int8_t*)(base + o.act);
+  w.scr = (double*)(base + o.scr); w.valid = (int*)(base + o.valid);
+  w.lk = (double*)(base + o.lk); w.M = (double*)(base + o.M);
+  w.state = d.wide ? base + o.state : nullptr;
+  w.dpump = (double*)(base + o.pump);
+  w.nscr = nscr;
+  return w;
+}
+
 }  // namespace
 
 struct WdsPlan {
@@ -95,6 +131,10 @@ struct WdsPlan {
   int nnzA_lower = 0;
   bool have_state = false;
   int state_batch = 0;
+  // changes with every call that rewrites the workspace (a forward, the
+  // unrolled reverse pass), so that a caller holding a pending backward can
+  // tell whether its kept state is still the plan's
+  int64_t gen = 0;
 };
 
 extern "C" const char* wds_last_error(void) { return g_err.c_str(); }
@@ -742,28 +782,16 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   plan->max_batch = max_batch;
   DevWork& w = plan->dw;
   // heads, rp, res, sx, 2p Woodbury columns, 2p+1 per-warp temporaries
-  w.nscr = 5 + 4 * std::max(npcv, 1);
-  const size_t B = (size_t)max_batch, pc = (size_t)std::max(npcv, 1);
-  size_t bytes = 0;
-  auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
-  size_t ow = take(B * nnzL * 8), op = take(B * L * 8), odr = take(B * L * 8),
-         oemh = take(B * Nj * 8), ohge = take(B * Nj * 8), odke = take(B * Nj * 8),
-         oact = take(B * pc), oscr = take(B * w.nscr * Nj * 8), oval = take(B * 4),
-         olk = take(B * 2 * L * 8), otop = take(B * std::max(nT * nT, 1) * 8),
-         ostate = take(d.wide ? B * state_bytes : 0), opump = take(B * 3 * npump * 8);
+  const int nscr = 5 + 4 * std::max(npcv, 1);
+  const WorkOff wo = work_layout(d, nscr, (size_t)max_batch, state_bytes);
+  const size_t bytes = wo.bytes;
   if (cudaMalloc(&plan->dwork, bytes) != cudaSuccess) {
     cudaFree(plan->dtab);
     delete plan;
     return fail(WDS_E_NOMEM, "wds_plan: cudaMalloc of the workspace failed");
   }
   cudaMemset(plan->dwork, 0, bytes);
-  unsigned char* wb = (unsigned char*)plan->dwork;
-  w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
-  w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
-  w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
-  w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
-  w.state = d.wide ? wb + ostate : nullptr;
-  w.dpump = (double*)(wb + opump);
+  w = work_at((unsigned char*)plan->dwork, wo, d, nscr);
   // ---- host copy of the symbolic structure
   HostSym& hs = plan->sym;
   hs.Nj = Nj; hs.perm = perm; hs.iperm = iperm; hs.parent = parent; hs.level = level;
@@ -777,6 +805,12 @@ extern "C" int wds_plan_stats(const WdsPlan* plan, int64_t* o) {
   o[0] = plan->dn.Nj; o[1] = plan->dn.nnzL; o[2] = plan->dn.nlev; o[3] = plan->dn.nfpair;
   o[4] = (int64_t)plan->smem_fwd; o[5] = plan->dn.npcv; o[6] = plan->nnzA_lower;
   o[7] = plan->groups;
+  return WDS_OK;
+}
+
+extern "C" int wds_state_generation(const WdsPlan* plan, int64_t* gen) {
+  if (!plan || !gen) return fail(WDS_E_ARG, "wds_state_generation: bad argument");
+  *gen = plan->gen;
   return WDS_OK;
 }
 
@@ -839,6 +873,7 @@ extern "C" int wds_forward(WdsPlan* plan, int32_t batch, const WdsForwardOpts* o
   if (rc != WDS_OK) return fail(rc, err);
   plan->have_state = o->polish_steps >= 0;
   plan->state_batch = batch;
+  ++plan->gen;
   return WDS_OK;
 }
 
@@ -909,6 +944,7 @@ extern "C" int wds_forward_multi(int32_t nplans, WdsPlan* const* plans, const in
   for (int p = 0; p < nplans; ++p) {
     plans[p]->have_state = opts[p].polish_steps >= 0;
     plans[p]->state_batch = batch[p];
+    ++plans[p]->gen;
   }
   return WDS_OK;
 }
@@ -1001,6 +1037,7 @@ extern "C" int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K,
   std::string err;
   const int rc = launch_unrolled(plan->dn, plan->dw, u, plan->groups, stream, &err);
   plan->have_state = false;  // the reverse pass reuses the plan's factor workspace
+  ++plan->gen;
   if (rc != WDS_OK) return fail(rc, err);
   return WDS_OK;
 }
@@ -1016,16 +1053,17 @@ extern "C" int wds_free(WdsPlan* plan) {
 // ---------------------------------------------------------------------------
 // Forward without allocation.
 //
-// Some callers cannot call cudaMalloc when they solve: a control loop that
-// must not touch the allocator after start-up (real-time pressure management,
-// where an allocation can stall for milliseconds), code recorded into a CUDA
-// graph by stream capture (where cudaMalloc is not allowed), or a host
-// process whose device memory is owned by another allocator.  For them,
-// wds_forward_noalloc runs the same forward kernel as wds_forward, but its
-// per-scenario workspace (the polish's heads and Woodbury columns, the
-// terminal factor and coefficients) lives in the fixed array below instead of
-// the plan's workspace.  The array is WDS_NOALLOC_SCRATCH_BYTES (64 MiB) and
-// every GPU that loads this library holds it until the process exits.
+// Some callers cannot call cudaMalloc when they solve: a pressure-management
+// control loop that allocates everything at start-up because an allocation
+// can stall it for milliseconds, or a host process whose device memory is
+// owned by another allocator (a simulator or framework that hands this
+// library only the buffers it asked for).  For them, wds_forward_noalloc runs
+// the same forward kernel as wds_forward, but its per-scenario workspace (the
+// polish's heads and Woodbury columns, the terminal factor and coefficients,
+// the link flows) lives in the fixed array below instead of the plan's
+// workspace, with the layout of work_layout.  The array is
+// WDS_NOALLOC_SCRATCH_BYTES (64 MiB) and every GPU that loads this library
+// holds it until the process exits.
 //
 // The kernel writes every word of the workspace it reads later in the same
 // call, so nothing needs clearing between calls; the array keeps the last
@@ -1036,26 +1074,19 @@ extern "C" int wds_free(WdsPlan* plan) {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[WDS_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-// Device address of g_noalloc_scratch per device (host code cannot use the
-// symbol itself: on the host it is only a stand-in, not a device address).
-constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
-std::mutex g_scratch_mu;
-
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the symbol is only a stand-in, not a device address, so it is looked up on
+// every call (cheap, and it allocates nothing): a cached address could
+// outlive the device context it came from (cudaDeviceReset).  The first
+// lookup on a device loads this library's device code there, which creates
+// the array.
 int scratch_address(void** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return fail(WDS_E_CUDA, "wds_forward_noalloc: no current CUDA device");
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (ce != cudaSuccess || !p)
-      return fail(WDS_E_CUDA, std::string("wds_forward_noalloc: cudaGetSymbolAddress: ") +
-                                  cudaGetErrorString(ce));
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (ce != cudaSuccess || !p)
+    return fail(WDS_E_CUDA, std::string("wds_forward_noalloc: cudaGetSymbolAddress: ") +
+                                cudaGetErrorString(ce));
+  *out = p;
   return WDS_OK;
 }
 }  // namespace
@@ -1074,20 +1105,11 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
     return fail(WDS_E_ARG, "wds_forward_noalloc: bad options");
   const DevNet& d = plan->dn;
   // the plan's workspace layout, for `batch` scenarios, inside the fixed array
-  const size_t B = (size_t)batch, pc = (size_t)std::max(d.npcv, 1);
-  const int nscr = plan->dw.nscr;
-  size_t bytes = 0;
-  auto take = [&](size_t n) { size_t off = bytes; bytes += (n + 255) / 256 * 256; return off; };
-  const size_t ow = take(B * d.nnzL * 8), op = take(B * d.L * 8), odr = take(B * d.L * 8),
-               oemh = take(B * d.Nj * 8), ohge = take(B * d.Nj * 8), odke = take(B * d.Nj * 8),
-               oact = take(B * pc), oscr = take(B * nscr * d.Nj * 8), oval = take(B * 4),
-               olk = take(B * 2 * d.L * 8), otop = take(B * std::max(d.nT * d.nT, 1) * 8),
-               ostate = take(d.wide ? B * state_smem_bytes(d) : 0),
-               opump = take(B * 3 * d.npump * 8);
-  if (bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
-    const size_t per = bytes / B;
+  const WorkOff wo = work_layout(d, plan->dw.nscr, (size_t)batch, state_smem_bytes(d));
+  if (wo.bytes > (size_t)WDS_NOALLOC_SCRATCH_BYTES) {
+    const size_t per = wo.bytes / (size_t)batch;
     return fail(WDS_E_ARG, "wds_forward_noalloc: batch " + std::to_string(batch) + " needs " +
-                               std::to_string(bytes) + " bytes of scratch, the fixed array holds " +
+                               std::to_string(wo.bytes) + " bytes of scratch, the fixed array holds " +
                                std::to_string((size_t)WDS_NOALLOC_SCRATCH_BYTES) +
                                " (at most " + std::to_string(WDS_NOALLOC_SCRATCH_BYTES / per) +
                                " scenarios of this network)");
@@ -1095,15 +1117,7 @@ extern "C" int wds_forward_noalloc(const WdsPlan* plan, int32_t batch, const Wds
   void* base = nullptr;
   int rc = scratch_address(&base);
   if (rc != WDS_OK) return rc;
-  unsigned char* wb = (unsigned char*)base;
-  DevWork w;
-  w.W = (double*)(wb + ow); w.P = (double*)(wb + op); w.dr = (double*)(wb + odr);
-  w.emh = (double*)(wb + oemh); w.hge = (double*)(wb + ohge); w.dke = (double*)(wb + odke);
-  w.act = (int8_t*)(wb + oact); w.scr = (double*)(wb + oscr); w.valid = (int*)(wb + oval);
-  w.lk = (double*)(wb + olk); w.M = (double*)(wb + otop);
-  w.state = d.wide ? wb + ostate : nullptr;
-  w.dpump = (double*)(wb + opump);
-  w.nscr = nscr;
+  const DevWork w = work_at((unsigned char*)base, wo, d, plan->dw.nscr);
   FwdArgs a{};
   a.B = batch; a.hacc = o->accuracy; a.max_iter = o->max_iter; a.sm = o->status_machine ? 1 : 0;
   a.refine = o->refine; a.polish = o->polish_steps; a.ke_stride = o->ke_stride;

@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from .autodiff import _adjoint_guards, _clamp_grh, _clamp_rhs
-from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
+from .solver import GGASolver, _Hold, _check_emitter_cap, _not_pd_hint
 
 __all__ = ["implicit_solve_multi", "solve_multi"]
 
@@ -133,6 +133,7 @@ class ImplicitMultiSM100(torch.autograd.Function):
             clamps.append(_adjoint_guards(s, o["flow"], o["status"], allow_clamp=True))
             res += [o["head"], o["flow"], o["emit"]]
         ctx.solvers, ctx.plans, ctx.clamps = solvers, plans, clamps
+        ctx.holds = [_Hold(pl) for pl in plans]   # kept until the backward
         ctx.B = [x[4] for x in ins]
         ctx.shapes = [(t.dim(), t.device) for t in tensors]
         return tuple(res)
@@ -142,6 +143,8 @@ class ImplicitMultiSM100(torch.autograd.Function):
         if torch.is_grad_enabled():
             raise NotImplementedError("implicit_solve_multi is first order only")
         solvers, plans = ctx.solvers, ctx.plans
+        for h in ctx.holds:
+            h.check("implicit_solve_multi backward")
         n = len(solvers)
         io = (_lib.WdsAdjointIO * n)()
         batch = (ctypes.c_int32 * n)()
@@ -174,6 +177,8 @@ class ImplicitMultiSM100(torch.autograd.Function):
         _lib.check(plans[0].lib.wds_adjoint_multi(n, handles, batch, io,
                                                   ctypes.c_void_p(cur.cuda_stream)),
                    "wds_adjoint_multi")
+        for h in ctx.holds:
+            h.release()
         for p in range(n):
             if fixes[p] is not None:
                 _clamp_grh(fixes[p], keep[3 * p + 1], outs[p][0], outs[p][1])

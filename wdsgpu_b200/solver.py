@@ -45,6 +45,7 @@ class _Plan:
         self.max_batch = int(max_batch)
         self.device = solver.device
         self.handle = ctypes.c_void_p()
+        self.held = False                  # a pending backward keeps its terminal state here
         t = solver._tables
         self._keep = t                     # host arrays must outlive wds_plan
         net = _lib.WdsNetwork()
@@ -104,6 +105,13 @@ class _Plan:
             _ptr(level, ctypes.c_int32)), "wds_plan_symbolic")
         return dict(perm=perm, colptr=colptr, rowidx=rowidx, parent=parent, level=level)
 
+    def generation(self):
+        """The plan's kept-state generation (`wds_state_generation`)."""
+        g = ctypes.c_int64()
+        _lib.check(self.lib.wds_state_generation(self.handle, ctypes.byref(g)),
+                   "wds_state_generation")
+        return int(g.value)
+
     def free(self):
         if self.handle:
             self.lib.wds_free(self.handle)
@@ -112,6 +120,44 @@ class _Plan:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class _Hold:
+    """A pending backward's claim on the plan that holds its terminal factor.
+
+    The reference keeps the factor of each forward in its own autograd
+    context (`ctx.kf`, dgga/autodiff.py:1203-1243), so two forwards before
+    their backwards each differentiate their own state.  Here the factor lives
+    in a plan's workspace: while a forward's backward is pending its plan is
+    held, and `GGASolver.plan` gives later forwards another plan.  The claim
+    ends with the backward or when the autograd graph is freed.  The plan's
+    state generation, recorded at the forward, is checked before the adjoint,
+    so a state that was replaced anyway (a second backward after the claim
+    ended and another forward ran) raises instead of giving a wrong gradient."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        self.gen = plan.generation()
+        self.active = True
+        plan.held = True
+
+    def check(self, who):
+        if self.plan.generation() != self.gen:
+            raise RuntimeError(
+                "%s: the terminal state of this forward was replaced by a later forward on "
+                "the same plan (backward after the graph's claim ended); run the forward "
+                "again" % who)
+
+    def release(self):
+        if self.active:
+            self.active = False
+            self.plan.held = False
+
+    def __del__(self):
+        try:
+            self.release()
         except Exception:
             pass
 
@@ -236,7 +282,7 @@ class GGASolver:
         self.node_ke_default = torch.as_tensor(np.asarray(net.node_ke, dtype=np.float64),
                                                device=self.device)
         self.r_hw = torch.as_tensor(np.asarray(net.r_hw, dtype=np.float64), device=self.device)
-        self._plans = {}
+        self._plans = []
 
     # ------------------------------------------------------------ set-up
     @staticmethod
@@ -445,18 +491,20 @@ class GGASolver:
 
     def plan(self, batch):
         """Plan (symbolic analysis + device tables + workspace) able to run
-        `batch` scenarios; plans are kept per capacity."""
+        `batch` scenarios: the smallest kept plan of enough capacity whose
+        terminal state no pending backward holds, else a new one (capacity a
+        power of two)."""
         if self.device.type != "cuda":
             raise NotImplementedError(
                 "linear_solver='sm100' needs a CUDA device (got %s)" % self.device)
-        for cap, p in self._plans.items():
-            if cap >= batch:
-                return p
+        free = [p for p in self._plans if p.max_batch >= batch and not p.held]
+        if free:
+            return min(free, key=lambda p: p.max_batch)
         cap = 1
         while cap < batch:
             cap *= 2
         p = _Plan(self, cap)
-        self._plans[cap] = p
+        self._plans.append(p)
         return p
 
     def plan_stats(self, batch=1):
