@@ -24,6 +24,8 @@ Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
         python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
         python tests/golden/make_golden.py unrolled (unrolled-K gradient pin, unrolled_ref.npz)
+        python tests/golden/make_golden.py cfg3   (the mixed-size workload's 100-junction and
+                                                   79-TCV networks, cfg3_small.npz / cfg3_tcv.npz)
 """
 import json
 import os
@@ -159,6 +161,11 @@ def main():
         ke = np.broadcast_to(net.node_ke, d.shape).copy()
         sens = synth.sensor_nodes(net, 6)
         cases[tag] = (net, d, rh, ke, sens, 1e-7, True, False)
+    write_cases(dgga, torch, cases)
+
+
+def write_cases(dgga, torch, cases):
+    """Run the reference on each case and write <tag>.npz."""
     for tag, (net, d, rh, ke, sens, acc, sm, ep) in cases.items():
         res = run_case(dgga, torch, net, d, rh, ke, sens, acc, sm, ep)
         blob = pack_net(net)
@@ -171,6 +178,28 @@ def main():
         print("%-9s iters=%s -> %s (%d KB)" % (
             tag, res["fwd_iters"].tolist(), os.path.basename(path),
             os.path.getsize(path) // 1024))
+
+
+def make_cfg3():
+    """The mixed-size workload's own networks, pinned one by one: the
+    100-junction looped network and the 542-junction network with 79 throttle
+    control valves (the Km / CSMALL valve branch, dgga/solver.py:2203-2219),
+    four scenarios each at the workload's lognormal(0.3) demand spread, with
+    the status machine."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    nets = synth.config3_networks()
+    cases = {}
+    for tag, net, seed in (("cfg3_small", nets[0], 61), ("cfg3_tcv", nets[1], 62)):
+        d, _ = synth.config2_scenarios(net, 4, seed=seed, sigma=0.3)
+        rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+        ke = np.broadcast_to(net.node_ke, d.shape).copy()
+        sens = synth.sensor_nodes(net, 8)
+        cases[tag] = (net, d, rh, ke, sens, 1e-6, True, False)
+    write_cases(dgga, torch, cases)
 
 
 def make_eps(T=6):
@@ -478,5 +507,7 @@ if __name__ == "__main__":
         make_psv()
     elif sys.argv[1:] == ["unrolled"]:
         make_unrolled()
+    elif sys.argv[1:] == ["cfg3"]:
+        make_cfg3()
     else:
         main()

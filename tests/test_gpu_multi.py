@@ -58,3 +58,43 @@ def test_multi_implicit_and_adjoint_equal_single_launches(mixed, cuda):
         ((h1 ** 2).sum() + (q1 ** 2).sum()).backward()
         assert torch.equal(h, h1) and torch.equal(q, q1)
         assert torch.equal(D.grad, D1.grad)
+
+
+def test_multi_matches_reference_goldens(cuda):
+    """The mixed-size workload's 100-junction and 79-TCV networks and the
+    782-junction network in one multi-plan launch, against the reference's own
+    outputs (tests/golden/cfg3_small.npz, cfg3_tcv.npz, cfg2.npz): iterations
+    and statuses exact, polished heads within 1e-9 m, gradients w.r.t.
+    demand, Ke and r within 1e-6 relative."""
+    from tests.golden.load import load
+    cases = [load(t) for t in ("cfg3_small", "cfg3_tcv", "cfg2")]
+    solvers = [GGASolver(net, device=cuda, dense_status_machine=True) for net, _, _ in cases]
+    acc = float(cases[0][1]["accuracy"])
+    assert all(float(inp["accuracy"]) == acc for _, inp, _ in cases)
+    fw = solve_multi(solvers, [inp["demand"] for _, inp, _ in cases],
+                     [inp["res_head"] for _, inp, _ in cases],
+                     kes=[inp["ke"] for _, inp, _ in cases], accuracy=acc, status_machine=True)
+    for (net, inp, ref), r in zip(cases, fw):
+        np.testing.assert_array_equal(r["iters"].cpu().numpy(), ref["fwd_iters"])
+        np.testing.assert_array_equal(r["status"].cpu().numpy(), ref["fwd_status"])
+        assert np.abs(r["head_ft"].cpu().numpy() - ref["fwd_head"]).max() < 1e-4
+    Ds = [torch.tensor(inp["demand"], device=cuda, requires_grad=True) for _, inp, _ in cases]
+    Ks = [torch.tensor(inp["ke"][0], device=cuda, requires_grad=True) for _, inp, _ in cases]
+    Rs = [torch.tensor(np.asarray(net.r_hw), device=cuda, requires_grad=True)
+          for net, _, _ in cases]
+    outs = implicit_solve_multi(solvers, Ds, [torch.tensor(inp["res_head"], device=cuda)
+                                              for _, inp, _ in cases],
+                                kes=Ks, r_hws=Rs, accuracy=acc)
+    loss = sum((h[:, inp["sensors"]] ** 2).sum() for (h, _, _), (_, inp, _) in zip(outs, cases))
+    loss.backward()
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    for (net, inp, ref), (h, q, e), D, K, R in zip(cases, outs, Ds, Ks, Rs):
+        assert np.abs(h.detach().cpu().numpy() - ref["imp_head"]).max() < 1e-9 / 0.3048
+        assert np.abs(q.detach().cpu().numpy() - ref["imp_flow"]).max() < 1e-9
+        assert rel(D.grad.cpu().numpy(), ref["grad_demand"]) < 1e-6
+        assert rel(R.grad.cpu().numpy(), ref["grad_r"]) < 1e-6
+        if np.abs(ref["grad_ke"]).max() > 0:
+            assert rel(K.grad.cpu().numpy(), ref["grad_ke"]) < 1e-6
