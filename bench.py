@@ -185,7 +185,7 @@ def run_reference(args, rank, world):
         return
     import multiprocessing as mp
     from wdsgpu_b200 import synth
-    cores = os.cpu_count() or 1
+    cores = physical_cores()            # SMT siblings counted once
     workers = max(1, min(cores, 32))
     net = synth.config2_network()
     d, rh = synth.config2_scenarios(net, 1024, seed=1000)
@@ -215,6 +215,147 @@ def run_reference(args, rank, world):
                                        % workers},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ the reference's own code
+def _reference_package():
+    """The unmodified reference (package `dgga`) installed offline into
+    baseline/_ref.  Its INP parser imports `wntr` at module top, which is not
+    installed; a stub with the imported names stands in (the parser is never
+    called: the network is built here and handed over as a `Net`)."""
+    import types
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "dgga")):
+        return None, "reference not installed in baseline/_ref"
+    if "wntr" not in sys.modules:
+        w = types.ModuleType("wntr")
+        ep = types.ModuleType("wntr.epanet")
+        ut = types.ModuleType("wntr.epanet.util")
+        ut.FlowUnits = type("FlowUnits", (), {})
+        nw = types.ModuleType("wntr.network")
+        el = types.ModuleType("wntr.network.elements")
+        for n in ("Junction", "Reservoir", "Tank", "Pipe", "Pump", "Valve"):
+            setattr(el, n, type(n, (), {}))
+        w.epanet, ep.util, w.network, nw.elements = ep, ut, nw, el
+        sys.modules.update({"wntr": w, "wntr.epanet": ep, "wntr.epanet.util": ut,
+                            "wntr.network": nw, "wntr.network.elements": el})
+    sys.path.insert(0, ref)
+    import dgga.autodiff
+    import dgga.parse
+    import dgga.solver
+    return dgga, None
+
+
+def physical_cores():
+    """Physical cores of this host (SMT siblings counted once)."""
+    try:
+        seen = set()
+        base = "/sys/devices/system/cpu"
+        for c in os.listdir(base):
+            f = os.path.join(base, c, "topology", "core_id")
+            g = os.path.join(base, c, "topology", "physical_package_id")
+            if c.startswith("cpu") and c[3:].isdigit() and os.path.exists(f):
+                seen.add((open(g).read().strip(), open(f).read().strip()))
+        if seen:
+            return len(seen)
+    except OSError:
+        pass
+    return os.cpu_count() or 1
+
+
+def run_reference_code(args):
+    """`--workload refgpu|refcpu`: the reference's own implementation of the
+    path, unmodified, through its public API (dgga/autodiff.py:1315-1351), on
+    the bench workload: GGASolver(mode="dense", dense_status_machine=True) and
+    implicit_solve(..., adjoint="gpu", accuracy=1e-6, status_machine=True),
+    the loss and gradients of the bench step.  refgpu: its GPU route on this
+    B200 at the full B (dense route: torch batched Cholesky; the cuDSS route
+    when nvmath is importable), device time per step with CUDA events around
+    the call, best-of and median as in scripts/mainline_v2/mv2_time_gpu.py:
+    72-87.  refcpu: the same route on the host cores (torch threads = physical
+    cores) on a sample of scenarios per step."""
+    import torch
+    from wdsgpu_b200 import synth
+    dgga, why = _reference_package()
+    gpu = args.workload == "refgpu"
+    if dgga is None:
+        print(json.dumps({"impl": "reference-code", "workload": args.workload,
+                          "unavailable": why}), flush=True)
+        return
+    try:
+        import nvmath  # noqa: F401
+        have_cudss = gpu
+    except ImportError:
+        have_cudss = False
+    cores = physical_cores()
+    if gpu:
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        B = args.batch
+    else:
+        dev = torch.device("cpu")
+        torch.set_num_threads(cores)
+        B = 16
+    net = synth.config2_network()
+    rnet = dgga.parse.Net(**net.as_fields())
+    s = dgga.solver.GGASolver(rnet, device=str(dev), dtype=torch.float64, mode="dense",
+                              dense_status_machine=True)
+    d_np, rh_np = synth.config2_scenarios(net, B, seed=1000)
+    sens = torch.as_tensor(synth.sensor_nodes(net, N_SENSORS), device=dev)
+    D0 = torch.as_tensor(d_np, device=dev)
+    RH = torch.as_tensor(rh_np, device=dev)
+    R0 = torch.as_tensor(np.asarray(net.r_hw), device=dev)
+    K0 = torch.as_tensor(np.asarray(net.node_ke), device=dev)
+    routes = [("dense", "dense")] + ([("csr", "cudss")] if have_cudss else [])
+    res = {}
+    for asm, ls in routes:
+        def step():
+            D = D0.clone().requires_grad_(True)
+            R = R0.clone().requires_grad_(True)
+            K = K0.clone().requires_grad_(True)
+            h, q, e = dgga.autodiff.implicit_solve(
+                s, D, RH, ke=K, r_hw=R, accuracy=ACCURACY, max_iter=200,
+                polish_steps=POLISH, adjoint="gpu", status_machine=True, assemble=asm,
+                linear_solver=ls)
+            (h.index_select(1, sens) ** 2).sum().backward()
+            return D.grad
+
+        ms = []
+        for i in range(max(1, args.warmup) + args.steps):
+            if gpu:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                step()
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1)
+            else:
+                t0 = time.perf_counter()
+                step()
+                t = 1e3 * (time.perf_counter() - t0)
+            if i >= max(1, args.warmup):
+                ms.append(t)
+        res[ls] = {"best_ms": min(ms), "median_ms": statistics.median(ms),
+                   "scenarios_per_s_best": B / (min(ms) / 1e3),
+                   "scenarios_per_s_median": B / (statistics.median(ms) / 1e3)}
+    main_route = "cudss" if "cudss" in res else "dense"
+    value = res[main_route]["scenarios_per_s_median"]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1 if gpu else 0,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res[main_route]["median_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference-code", "workload": args.workload,
+            "config": {"workload": WORKLOAD.replace("B=1024", "B=%d" % B), "B": B,
+                       "route": "%s/%s" % ("csr" if main_route == "cudss" else "dense",
+                                           main_route),
+                       "cudss": "available" if have_cudss else
+                                "unavailable on this box (nvmath not installed)",
+                       "device": torch.cuda.get_device_name(0) if gpu else "host cpu",
+                       "torch_threads": None if gpu else cores},
+            "routes": res}
     print(json.dumps(line), flush=True)
 
 
@@ -340,6 +481,47 @@ def run_secondary(args):
     print(json.dumps(line), flush=True)
 
 
+def fp32_form(net, d_dev, rh_dev, sens, B):
+    """The same step with the FP32 factor and FP64 refinement
+    (sm100_factor_dtype = float32): its time per step and its head and
+    gradient differences from the FP64 form, or the refusal it raises."""
+    import torch
+    from wdsgpu_b200.autodiff import implicit_solve
+    from wdsgpu_b200.solver import GGASolver
+    out = {}
+    for name, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        s = GGASolver(net, device=d_dev.device, dense_status_machine=True)
+        s.sm100_factor_dtype = dt
+        try:
+            D = d_dev.clone().requires_grad_(True)
+            h = implicit_solve(s, D, rh_dev, accuracy=ACCURACY, polish_steps=POLISH,
+                               status_machine=True)[0]
+            (h.index_select(1, sens) ** 2).sum().backward()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            D2 = d_dev.clone().requires_grad_(True)
+            h2 = implicit_solve(s, D2, rh_dev, accuracy=ACCURACY, polish_steps=POLISH,
+                                status_machine=True)[0]
+            (h2.index_select(1, sens) ** 2).sum().backward()
+            e1.record()
+            torch.cuda.synchronize()
+            out[name] = {"ms": e0.elapsed_time(e1), "head": h2.detach(), "grad": D2.grad}
+        except RuntimeError as exc:
+            out[name] = {"refused": str(exc)[:200]}
+    res = {"fp64_scenarios_per_s": B / (out["fp64"]["ms"] / 1e3)}
+    if "refused" in out["fp32"]:
+        res["fp32"] = "refused: " + out["fp32"]["refused"]
+    else:
+        g64, g32 = out["fp64"]["grad"], out["fp32"]["grad"]
+        res.update({"fp32_scenarios_per_s": B / (out["fp32"]["ms"] / 1e3),
+                    "max_head_diff_m": float((out["fp32"]["head"] - out["fp64"]["head"])
+                                             .abs().max()) * 0.3048,
+                    "grad_rel_diff": float((g32 - g64).abs().max() / g64.abs().max())})
+    return res
+
+
 # ------------------------------------------------------------------ GPU leg
 def main():
     ap = argparse.ArgumentParser()
@@ -349,11 +531,17 @@ def main():
     ap.add_argument("--impl", default="sm100", choices=("sm100", "reference"))
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=("config2", "mixed", "eps", "unrolled"))
+    ap.add_argument("--workload", default="config2",
+                    choices=("config2", "config4", "mixed", "eps", "unrolled", "refgpu", "refcpu"))
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload != "config2":
+    if args.workload in ("refgpu", "refcpu"):
+        run_reference_code(args)
+        return
+    if args.workload == "config4":
+        args.batch = 16384 if args.batch == 1024 else args.batch
+    elif args.workload != "config2":
         run_secondary(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,17 +581,19 @@ def main():
     ke_dev = s.node_ke_default.clone()
     stream = torch.cuda.current_stream(dev)
 
-    def step(D, R, KE):
+    def step(D, R, KE, RH=None, full=False):
         D = D.detach().requires_grad_(True)
         R = R.detach().requires_grad_(True)
         KE = KE.detach().requires_grad_(True)
-        h, q, e = implicit_solve(s, D, rh_dev, ke=KE, r_hw=R, accuracy=ACCURACY,
-                                 polish_steps=POLISH, status_machine=True)
+        h, q, e = implicit_solve(s, D, rh_dev if RH is None else RH, ke=KE, r_hw=R,
+                                 accuracy=ACCURACY, polish_steps=POLISH, status_machine=True)
         loss = (h.index_select(1, sens) ** 2).sum()
         loss.backward()
         gR, gK = R.grad, KE.grad
         allreduce_batch_summed([gR, gK])
         gC = gR * dC
+        if full:   # the plugin call's whole result: state and gradients
+            return loss.detach(), D.grad, gC, gK, h.detach(), q.detach()
         return loss.detach(), D.grad, gC, gK
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -442,12 +632,19 @@ def main():
     fwd_ms = [a.elapsed_time(b) for (nm, a, b) in events if nm == "forward"]
     adj_ms = [a.elapsed_time(b) for (nm, a, b) in events if nm == "adjoint"]
     # ---- end to end through the public API with host buffers
+    # every input of the call goes host -> device (demand, reservoir heads,
+    # roughness-derived resistances, emitter coefficients), and the whole
+    # result comes back: loss, gradients w.r.t. demand, C and Ke, heads, flows
     d_host = torch.as_tensor(d_np).pin_memory()
+    rh_host = torch.as_tensor(rh_np).pin_memory()
     r_host = r_dev.cpu().pin_memory()
+    ke_host = ke_dev.cpu().pin_memory()
     outs = [torch.empty(1, dtype=torch.float64).pin_memory(),
             torch.empty(B, net.N, dtype=torch.float64).pin_memory(),
             torch.empty(net.L, dtype=torch.float64).pin_memory(),
-            torch.empty(net.N, dtype=torch.float64).pin_memory()]
+            torch.empty(net.N, dtype=torch.float64).pin_memory(),
+            torch.empty(B, net.N, dtype=torch.float64).pin_memory(),
+            torch.empty(B, net.L, dtype=torch.float64).pin_memory()]
     e2e_ms = []
     barrier()
     for i in range(args.warmup + args.steps):
@@ -456,9 +653,11 @@ def main():
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         Dd = d_host.to(dev, non_blocking=True)
+        RHd = rh_host.to(dev, non_blocking=True)
         Rd = r_host.to(dev, non_blocking=True)
-        loss, gD, gC, gK = step(Dd, Rd, ke_dev)
-        for o, g in zip(outs, (loss.reshape(1), gD, gC, gK)):
+        KEd = ke_host.to(dev, non_blocking=True)
+        loss, gD, gC, gK, hh, qq = step(Dd, Rd, KEd, RH=RHd, full=True)
+        for o, g in zip(outs, (loss.reshape(1), gD, gC, gK, hh, qq)):
             o.copy_(g, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
@@ -469,7 +668,7 @@ def main():
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t)
-    h2d = d_host.numel() * 8 + r_host.numel() * 8
+    h2d = sum(x.numel() * 8 for x in (d_host, rh_host, r_host, ke_host))
     d2h = sum(o.numel() * 8 for o in outs)
     # ---- roofline of the dominant kernel (the fused forward)
     st = s.plan_stats(B)
@@ -516,6 +715,11 @@ def main():
                                   % (bpi, rg, bpi2, POLISH + 1)},
             "clocks": clk.summary(),
         }
+        if args.workload == "config4":
+            line["metric"] = ("fwd+adjoint scenarios/s at B=16384 (782 jn), FP64 factor; "
+                              "FP32 factor + FP64 refinement form beside it")
+            line["config"]["workload"] = ("large batch: " + line["config"]["workload"])
+            line["fp32_form"] = fp32_form(s.net, d_dev, rh_dev, sens, B)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline_single()
         print(json.dumps(line), flush=True)

@@ -172,6 +172,23 @@ typedef struct WdsForwardOpts {
    * each iteration's starting flows, emitter flows (by junction) and
    * solved junction heads there, for wds_unrolled_adjoint. */
   double* unroll_record;
+  /* Condition proxy of GGASolver.solve's result dict (`diag_ratio`,
+   * dgga/solver.py:3026-3032, 3205-3207): a device array [B] or NULL; per
+   * scenario max |A_jj| / max(min |A_jj|, 1e-300) of the node matrix
+   * assembled in its last GGA iteration (PRV valve coefficients and the CBIG
+   * diagonal of ACTIVE valves included).  Written for networks with
+   * status-machine PRVs/PSVs, zero otherwise. */
+  double* diag_ratio;
+  /* Status-machine schedule (record_schedule, dgga/solver.py:2740-2745,
+   * 3136-3160): device arrays, zero on entry, or NULL.  sched_flags uint8
+   * [B][T] (T = max_iter + max(extra_iter, 0)): bit 2 when the scenario ran
+   * iteration t + 1, bit 0 when that iteration ran the link-status check on
+   * the converged branch, bit 1 on the periodic branch; sched_chg uint32
+   * [B][T][ceil(L / 32)]: bit k of a row set when the iteration's valve
+   * status pass (PRV/PSV links) or link-status check (the other links)
+   * changed link k's status. */
+  uint8_t* sched_flags;
+  uint32_t* sched_chg;
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;

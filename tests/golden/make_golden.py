@@ -24,6 +24,9 @@ Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
         python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
         python tests/golden/make_golden.py unrolled (unrolled-K gradient pin, unrolled_ref.npz)
+        python tests/golden/make_golden.py valves (8 PRVs + 2 PSVs on one network, valves_ref.npz)
+        python tests/golden/make_golden.py contract (diag_ratio and record_schedule of solve(),
+                                                   contract_ref.npz)
         python tests/golden/make_golden.py cfg3   (the mixed-size workload's 100-junction and
                                                    79-TCV networks, cfg3_small.npz / cfg3_tcv.npz)
 """
@@ -450,6 +453,68 @@ def make_psv():
     _valve_case(dgga, torch, net, d, rh, np.flatnonzero((lt == 3) | (lt == 4)), "psv_ref")
 
 
+def make_valves():
+    """Many-valve pin: eight PRV zones and two PSVs on one 520-junction
+    network, four scenarios, every valve ACTIVE in most of them (ten
+    constraint rows in the polish and the adjoint; the reference's valve loop
+    and Woodbury take any count, dgga/solver.py:863, dgga/autodiff.py:
+    965-1029).  The EPANET replica with its status machine and the CPU
+    adjoint, as for the PSV pin (the reference's dense route refuses PSVs)."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.many_valves_network()
+    d, _ = synth.config2_scenarios(net, 4, seed=31, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    lt = np.asarray(net.link_type)
+    _valve_case(dgga, torch, net, d, rh, np.flatnonzero((lt == 3) | (lt == 4)), "valves_ref")
+
+
+def make_contract():
+    """The rest of solve()'s result contract on the golden inputs: the
+    condition proxy `diag_ratio` (dgga/solver.py:3026-3032, 3205-3207) and
+    the status-machine schedule of record_schedule=True (:2740-2745,
+    3154-3160), from the reference's dense batched route, for the cfg2,
+    feat_mid, feat_low and cfg3_tcv cases.  Writes contract_ref.npz with
+    <tag>__diag_ratio and <tag>__sched_{it,valve,a,b,chg} arrays (one row per
+    schedule entry: a valve-pass entry has valve = True, a = act; a
+    link-status entry a = conv, b = per)."""
+    import torch
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.dirname(HERE))
+    from golden.load import load
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    blob = {}
+    for tag in ("cfg2", "feat_mid", "feat_low", "cfg3_tcv"):
+        net, inp, _ = load(tag)
+        ref_net = dgga.parse.Net(**net.as_fields())
+        sd = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense",
+                                   dense_status_machine=True)
+        f = sd.solve(torch.tensor(inp["demand"]), torch.tensor(inp["res_head"]),
+                     ke_int=torch.tensor(inp["ke"]), status_machine=True,
+                     accuracy=float(inp["accuracy"]), assemble="csr", linear_solver="dense",
+                     record_schedule=True)
+        if "diag_ratio" in f:
+            blob[tag + "__diag_ratio"] = f["diag_ratio"].numpy()
+        sch = f["schedule"]
+        B = inp["demand"].shape[0]
+        blob[tag + "__sched_it"] = np.array([e["it"] for e in sch], dtype=np.int64)
+        blob[tag + "__sched_valve"] = np.array([e.get("kind") == "valve" for e in sch])
+        blob[tag + "__sched_a"] = np.stack([np.asarray(e["act"] if e.get("kind") == "valve"
+                                                       else e["conv"]) for e in sch]).astype(bool)
+        blob[tag + "__sched_b"] = np.stack([np.asarray(e["per"]) if "per" in e
+                                            else np.zeros(B, bool) for e in sch]).astype(bool)
+        blob[tag + "__sched_chg"] = np.stack([e["chg"] for e in sch]).astype(bool)
+        print("%-9s schedule iterations %s, changes %d, diag_ratio %s" % (
+            tag, blob[tag + "__sched_it"].tolist(), int(blob[tag + "__sched_chg"].sum()),
+            None if "diag_ratio" not in f else f["diag_ratio"].numpy().round(1).tolist()))
+    path = os.path.join(HERE, "contract_ref.npz")
+    np.savez_compressed(path, **blob)
+
+
 def make_unrolled():
     """Unrolled-K pin: the reference's solve_unrolled (dgga/autodiff.py:
     1357-1664, K = 8 fixed GGA iterations, statuses frozen at the initial
@@ -509,5 +574,9 @@ if __name__ == "__main__":
         make_unrolled()
     elif sys.argv[1:] == ["cfg3"]:
         make_cfg3()
+    elif sys.argv[1:] == ["valves"]:
+        make_valves()
+    elif sys.argv[1:] == ["contract"]:
+        make_contract()
     else:
         main()

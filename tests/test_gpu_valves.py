@@ -21,7 +21,7 @@ from oracle.gga import Model  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref"])
+@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref", "valves_ref"])
 def test_valve_forward_matches_reference(cuda, case):
     from wdsgpu_b200.solver import GGASolver
     net, inp, ref = load(case)
@@ -34,7 +34,7 @@ def test_valve_forward_matches_reference(cuda, case):
     assert np.abs(out["head_ft"].cpu().numpy() - ref["fwd_head"]).max() < 1e-4
 
 
-@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref"])
+@pytest.mark.parametrize("case", ["fcv_ref", "psv_ref", "valves_ref"])
 def test_valve_gradients_match_reference(cuda, case):
     from wdsgpu_b200.autodiff import implicit_solve
     from wdsgpu_b200.solver import GGASolver
@@ -58,12 +58,13 @@ def test_valve_gradients_match_reference(cuda, case):
         assert np.abs(gi - Rf).max() <= 1e-8 * np.abs(Rf).max(), (key, np.abs(gi - Rf).max())
 
 
-@pytest.mark.parametrize("which", ["fcv", "psv"])
+@pytest.mark.parametrize("which", ["fcv", "psv", "valves"])
 def test_valve_unseen_scenarios_against_oracle(cuda, which):
     from wdsgpu_b200 import synth
     from wdsgpu_b200.autodiff import implicit_solve
     from wdsgpu_b200.solver import GGASolver
-    net = synth.fcv_network() if which == "fcv" else synth.psv_network()
+    net = {"fcv": synth.fcv_network, "psv": synth.psv_network,
+           "valves": synth.many_valves_network}[which]()
     d, _ = synth.config2_scenarios(net, 12, seed=97, sigma=0.4)
     rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
     s = GGASolver(net, device=cuda, dense_status_machine=True)

@@ -58,7 +58,7 @@ def test_solve_argument_guards():
         s.solve(d, rh, assemble="dense", linear_solver="sm100")
     with pytest.raises(NotImplementedError):
         s.solve(d, rh, status_machine=True)       # needs dense_status_machine
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):           # the reference: dense status machine only
         s.solve(d, rh, record_schedule=True)
 
 

@@ -75,3 +75,27 @@ def test_oracle_psv_matches_reference():
                           (g[3], "g_rhw", slice(None)), (g[1], "g_res_head", fixed)):
         R = ref[key][:, cols]
         assert np.abs(gi[:, cols] - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi[:, cols] - R).max())
+
+
+def test_oracle_many_valves_match_reference():
+    """Eight PRVs and two PSVs on one network (fixture
+    tests/golden/valves_ref.npz): ten constraint rows, any valve count as in
+    the reference's valve loop and Woodbury (dgga/solver.py:863,
+    dgga/autodiff.py:965-1029)."""
+    net, inp, ref = load("valves_ref")
+    lt = np.asarray(net.link_type)
+    assert (lt == 3).sum() == 8 and (lt == 4).sum() == 2
+    out = Model(net).solve(inp["demand"], inp["res_head"], ke=inp["ke"], accuracy=1e-7,
+                           status_machine=True)
+    np.testing.assert_array_equal(out["iters"], ref["fwd_iters"].ravel())
+    np.testing.assert_array_equal(out["status"], ref["fwd_status"])
+    assert np.abs(out["head_ft"] - ref["fwd_head"]).max() < 1e-4
+    v = np.flatnonzero((lt == 3) | (lt == 4))
+    assert (ref["fwd_status"][:, v] == 4).sum() >= 35            # nearly every valve ACTIVE
+    out, g = valve_loss_grads(Model(net), net, inp)
+    assert np.abs(out["head_ft"] - ref["head"]).max() < 1e-9
+    fixed = np.asarray(net.node_type) != 0
+    for gi, key, cols in ((g[0], "g_demand", slice(None)), (g[2], "g_ke", slice(None)),
+                          (g[3], "g_rhw", slice(None)), (g[1], "g_res_head", fixed)):
+        R = ref[key][:, cols]
+        assert np.abs(gi[:, cols] - R).max() <= 1e-8 * np.abs(R).max(), (key, np.abs(gi[:, cols] - R).max())

@@ -189,6 +189,27 @@ __device__ void block_sum(double* v, int m, double* red) {
   }
 }
 
+// Group maximum of mx and minimum of mn (warp butterflies, then the warps'
+// values in order); every thread gets both results.
+template <int NT>
+__device__ void block_maxmin(double& mx, double& mn, double* red) {
+  for (int o = 16; o; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  }
+  const int w = gtid<NT>() >> 5, l = threadIdx.x & 31;
+  gsync<NT>();
+  if (l == 0) {
+    red[w * 4] = mx;
+    red[w * 4 + 1] = mn;
+  }
+  gsync<NT>();
+  for (int ww = 0; ww < NT / 32; ++ww) {
+    mx = fmax(mx, red[ww * 4]);
+    mn = fmin(mn, red[ww * 4 + 1]);
+  }
+}
+
 // ---------------------------------------------------------------- formulas
 // emitterheadloss (dgga/solver.py:2368-2377)
 __device__ __forceinline__ void emitter_hl(const DevNet& n, double e, double ke, double& hl,
@@ -1082,7 +1103,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
   // x <- x - sum_b z_b (X_b - e_jc_b),  z = C^{-1} (x[jc] act)
   auto wood = [&](double* x) {
     if (tid == 0) {
-      double Cc[16];
+      double* Cc = C + p * p;  // working copy (the small buffer holds 4 p^2 for C)
       for (int i = 0; i < p * p; ++i) Cc[i] = C[i];
       for (int a0 = 0; a0 < p; ++a0) y[a0] = x[n.pcv_jc[a0]] * actf[a0];
       dense_solve(Cc, y, p);
@@ -1301,6 +1322,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
   int nextcheck = n.checkfreq;
   int iters = maxtrials + 1, info = WDS_INFO_UNCONVERGED;
   double relerr = 0.0;
+  double dratio = 0.0;  // diag_ratio of the last iteration's assembled matrix
   const int rec_w = n.L + 2 * n.Nj;  // unrolled record: q [L], e [Nj], H [Nj] per iteration
   double* recb = a.rec ? a.rec + (size_t)b * maxtrials * rec_w : nullptr;
   for (int it = 1; it <= (em_ok ? maxtrials : 0); ++it) {
@@ -1319,6 +1341,16 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     }
     gsync<NT>();
     assemble_gga<NT, FT>(n, T, s, kerow, drow);
+    if (a.diag && n.npcv > 0) {  // condition proxy (dgga/solver.py:3026-3032)
+      double mx = 0.0, mn = kINF;
+      for (int p = gtid<NT>(); p < n.Nj; p += NT) {
+        const double dv = fabs((double)wp<FT>(s)[T.colptr[p]]);
+        mx = fmax(mx, dv);
+        mn = fmin(mn, dv);
+      }
+      block_maxmin<NT>(mx, mn, s.red);
+      dratio = mx / fmax(mn, 1e-300);
+    }
     if (!factor<NT, FT>(n, T, s)) {
       info = WDS_INFO_NOT_PD;
       iters = it;
@@ -1395,7 +1427,12 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
              : ((h1 < hs - ht && h1 > h2 + ht) ? WDS_OPEN : WDS_CLOSED);
       else if (sk == WDS_XPRESSURE)
         ns = neg ? WDS_CLOSED : sk;
-      if (ns != sk) vchg = true;
+      if (ns != sk) {
+        vchg = true;
+        if (a.schg)  // schedule record: the valve pass changed link k
+          atomicOr(&a.schg[((size_t)b * maxtrials + (it - 1)) * ((n.L + 31) >> 5) + (k >> 5)],
+                   1u << (k & 31));
+      }
       s.S[k] = (int8_t)ns;
     }
     vchg = gsync_or<NT>(vchg);
@@ -1451,11 +1488,18 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
           const bool cut_e = (fl & WDS_TL_IS_PUMP) ? (fl & WDS_TL_PUMP_OUT) != 0 : !cl_closed;
           if (live && ((full && cut_f) || (empty && cut_e))) st = WDS_TEMPCLOSED;
         }
-        if (st != st0) chg = true;
+        if (st != st0) {
+          chg = true;
+          if (a.schg)  // schedule record: link k changed in this check
+            atomicOr(&a.schg[((size_t)b * maxtrials + (it - 1)) * ((n.L + 31) >> 5) + (k >> 5)],
+                     1u << (k & 31));
+        }
         s.S[k] = (int8_t)st;
       }
       chg = gsync_or<NT>(chg);
     }
+    if (a.sflags && gtid<NT>() == 0)  // iteration it ran, and which link-status branch
+      a.sflags[(size_t)b * maxtrials + (it - 1)] = 4 | (br_conv ? 1 : 0) | (br_per ? 2 : 0);
     const bool stat_change = br_conv && (chg || vchg);
     if (br_conv && stat_change) nextcheck = it + n.checkfreq;
     if (br_per) nextcheck += n.checkfreq;
@@ -1621,6 +1665,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     a.iters[b] = iters;
     a.relerr[b] = relerr;
     a.info[b] = info;
+    if (a.diag) a.diag[b] = dratio;
   }
 }
 
@@ -1726,7 +1771,7 @@ __device__ __forceinline__ void adjoint_one(const DevNet& n, const DevWork& w, c
     gsync<NT>();
     auto wood = [&](double* x, const double* rr) {
       if (gtid<NT>() == 0) {
-        double Cc[64];
+        double* Cc = actf + p;  // working copy, p^2 after C, y, actf in the small buffer
         for (int i = 0; i < p * p; ++i) Cc[i] = C[i];
         for (int a0 = 0; a0 < p; ++a0)
           y[a0] = (x[n.pcv_jc[a0]] - x[n.pcv_jo[a0]] - rr[n.pcv_jc[a0]]) * actf[a0];

@@ -173,6 +173,9 @@ struct FwdArgs {
   int* iters;
   double* relerr;
   int* info;
+  double* diag;           // [B] diag_ratio, or null
+  uint8_t* sflags;        // [B][maxtrials] schedule branch flags, or null
+  uint32_t* schg;         // [B][maxtrials][ceil(L/32)] schedule change bits, or null
 };
 
 struct AdjArgs {

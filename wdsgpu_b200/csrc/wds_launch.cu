@@ -90,10 +90,6 @@ int launch_forward_multi(FwdJobs& jobs, void* stream, std::string* err) {
   bool fp32 = false;
   for (int p = 0; p < jobs.n; ++p) {
     FwdJob& J = jobs.j[p];
-    if (J.n.npcv > 4) {
-      *err = "wds_forward_multi: more than 4 status-machine PRVs is not supported by this build";
-      return WDS_E_UNSUPPORTED;
-    }
     if (p > 0 && (J.n.fp32 != 0) != fp32) {
       *err = "wds_forward_multi: the plans mix FP32 and FP64 factors";
       return WDS_E_ARG;
@@ -127,10 +123,6 @@ int launch_adjoint_multi(AdjJobs& jobs, void* stream, std::string* err) {
 
 int launch_forward(const DevNet& n, const DevWork& w, const FwdArgs& a, int groups,
                    void* stream, std::string* err) {
-  if (n.npcv > 4) {
-    *err = "wds_forward: more than 4 status-machine PRVs is not supported by this build";
-    return WDS_E_UNSUPPORTED;
-  }
   const void* kern = n.fp32 ? forward_kernel_f32(n.wide, groups) : forward_kernel_f64(n.wide, groups);
   return launch_single(kern, n, w, a, a.B, n.wide ? 1 : groups, stream, "wds_forward", err);
 }
@@ -144,10 +136,6 @@ int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int 
 
 int launch_adjoint(const DevNet& n, const DevWork& w, const AdjArgs& a, int groups,
                    void* stream, std::string* err) {
-  if (n.npcv > 4) {
-    *err = "wds_adjoint: more than 4 status-machine PRVs is not supported by this build";
-    return WDS_E_UNSUPPORTED;
-  }
   const void* kern = n.fp32 ? adjoint_kernel_f32(n.wide, groups) : adjoint_kernel_f64(n.wide, groups);
   return launch_single(kern, n, w, a, a.B, n.wide ? 1 : groups, stream, "wds_adjoint", err);
 }

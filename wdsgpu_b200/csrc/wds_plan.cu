@@ -835,6 +835,13 @@ static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::
     return fail(WDS_E_ARG, who + ": refine_band must be >= 0");
   a.rband = o->refine_band;
   a.rec = o->unroll_record;
+  a.diag = o->diag_ratio;
+  a.sflags = o->sched_flags;
+  a.schg = o->sched_chg;
+  if ((a.sflags == nullptr) != (a.schg == nullptr))
+    return fail(WDS_E_ARG, who + ": sched_flags and sched_chg go together");
+  if (a.sflags && !o->status_machine)
+    return fail(WDS_E_ARG, who + ": the schedule record needs status_machine 1");
   if (a.rec && (o->status_machine || o->polish_steps >= 0))
     return fail(WDS_E_ARG, who + ": the unrolled mode runs with status_machine 0 and no polish");
   a.th_sp = o->pump_speed;

@@ -578,8 +578,10 @@ class GGASolver:
                 raise NotImplementedError(
                     "this network has PRVs/PSVs/FCVs with a setting: solve(..., "
                     "status_machine=True) is required")
-        if record_schedule:
-            raise NotImplementedError("record_schedule is not provided by the sm100 route")
+        if record_schedule and not status_machine:
+            raise ValueError(
+                "record_schedule=True covers the batched status machine only "
+                "(status_machine=True), as in the reference")
 
     def refine_steps(self):
         """Refinement steps of a refined GGA solve (`sm100_refine`)."""
@@ -631,12 +633,14 @@ class GGASolver:
 
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
             refine=None, plan=None, q0=None, e0=None, pumps=None, refine_band=None,
-            record=None):
+            record=None, schedule=False):
         """One wds_forward call on device tensors; returns the raw outputs.
         q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
         warm start of GGASolver.solve (dgga/solver.py:2876-2887); pumps is
         the (speed, h0, r) of `pump_rows` (the call's pump parameters, or
-        None for the network's)."""
+        None for the network's).  The result holds `diag_ratio` [B] on networks
+        with status-machine PRVs/PSVs, and with schedule=True the raw schedule
+        record (`sched_flags`, `sched_chg`) for `_schedule`."""
         p = plan or self.plan(B)
         dev = self.device
         head = torch.empty(B, self.N, dtype=torch.float64, device=dev)
@@ -654,6 +658,16 @@ class GGASolver:
         o.refine_band = float(self.refine_band(hacc) if refine_band is None else refine_band)
         if record is not None:   # unrolled mode: max_iter iterations, recorded
             o.unroll_record = record.data_ptr()
+        diag = None
+        if self.n_pcv:
+            diag = torch.zeros(B, dtype=torch.float64, device=dev)
+            o.diag_ratio = diag.data_ptr()
+        sflags = schg = None
+        if schedule:
+            T = int(max_iter) + max(int(self.extra_iter), 0)
+            sflags = torch.zeros(B, T, dtype=torch.uint8, device=dev)
+            schg = torch.zeros(B, T, (self.L + 31) // 32, dtype=torch.int32, device=dev)
+            o.sched_flags, o.sched_chg = sflags.data_ptr(), schg.data_ptr()
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
@@ -683,7 +697,32 @@ class GGASolver:
         if ev is not None:
             ev[1].record(cur)
         return dict(head=head, flow=flow, emit=emit, status=status, iters=iters,
-                    relerr=relerr, info=info, plan=p, pumps=pumps)
+                    relerr=relerr, info=info, plan=p, pumps=pumps, diag_ratio=diag,
+                    sched_flags=sflags, sched_chg=schg)
+
+    def _schedule(self, flags, chg):
+        """The schedule list of the reference (dgga/solver.py:3136-3160): per
+        iteration that any scenario ran, on networks with status-machine
+        valves, dict(it, kind="valve", act[B], chg[B,L]) for the valve status
+        pass, then, when any scenario ran the link-status check,
+        dict(it, conv[B], per[B], chg[B,L])."""
+        fl = flags.cpu().numpy()
+        bits = chg.cpu().numpy().view(np.uint8)
+        valve = np.zeros(self.L, dtype=bool)
+        valve[self.pcv_links] = True
+        out = []
+        for t in np.flatnonzero((fl & 4).any(0)):
+            act = (fl[:, t] & 4) != 0
+            conv = (fl[:, t] & 1) != 0
+            per = (fl[:, t] & 2) != 0
+            c = np.unpackbits(bits[:, t, :], axis=1, bitorder="little")[:, :self.L].astype(bool)
+            if self.n_pcv:
+                out.append(dict(it=int(t) + 1, kind="valve", act=act,
+                                chg=c & valve[None, :] & act[:, None]))
+            if (conv | per).any():
+                out.append(dict(it=int(t) + 1, conv=conv, per=per,
+                                chg=c & ~valve[None, :] & (conv | per)[:, None]))
+        return out
 
     def solve(self, demand_cfs, res_head_ft, ke_int=None, q0=None, e0=None,
               max_iter=None, accuracy=None, link_status=None, link_setting=None,
@@ -704,7 +743,8 @@ class GGASolver:
         max_iter = self.max_iter_default if max_iter is None else int(max_iter)
         hacc = self.hacc_default if accuracy is None else float(accuracy)
         sm = bool(status_machine)
-        o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1, q0=q0, e0=e0)
+        o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1, q0=q0, e0=e0,
+                     schedule=bool(record_schedule))
         info = o["info"]
         _check_emitter_cap(self, info)
         bad = torch.nonzero(info & _lib.INFO_NOT_PD).flatten()
@@ -720,8 +760,12 @@ class GGASolver:
         else:
             self._check_pump_shutoff(o["head"], o["flow"])
             self._check_tank_status(o["head"], o["flow"])
+        if o["diag_ratio"] is not None:
+            out["diag_ratio"] = o["diag_ratio"]
         if single:
             out = {k: v[0] for k, v in out.items()}
+        if record_schedule:   # a list, not batched
+            out["schedule"] = self._schedule(o["sched_flags"], o["sched_chg"])
         return out
 
     def _warm(self, x, B, cols):

@@ -691,3 +691,89 @@ def tanks_as_junctions(net):
               "tank_vmax"):
         f[k] = np.zeros(0)
     return Net(**f)
+
+
+def many_valves_network(seed=8, n_prv=8, psv_links=2, psv_margin_m=12.0,
+                        psv_setting_m=(51.57, 48.71), psv_flip=(False, False),
+                        psv_pick=(293, 316)):
+    """Looped network with `n_prv` PRV zones (each a subtree fed only by its
+    PRV) and `psv_links` pressure sustaining valves on junction-to-junction
+    tree pipes of the main zone, oriented with the tree flow; each PSV's
+    setting is the static pressure at its upstream junction (highest
+    reservoir head minus elevation) less `psv_margin_m`, so that the
+    headloss upstream makes it throttle in most scenarios, unless the
+    settings (m, one per PSV in link order) are given; `psv_flip` (one bool
+    per PSV) reverses a PSV's orientation, for one that carries its flow
+    against the tree direction; `psv_pick` names the PSV links instead of
+    the seeded choice.  The defaults place both PSVs where, with settings
+    1 m above the pressure the pipe would see, they throttle (ACTIVE) in the
+    seeded lognormal(0.3) scenarios, next to eight ACTIVE PRVs: ten
+    constraint rows in the polish and the adjoint."""
+    net = looped_network(seed, n_junc=520, n_res=2, n_pipes=600, n_prv=n_prv,
+                         zone_size=(12, 40), prv_setting_m=(25.0, 40.0))
+    f = net.as_fields()
+    lt = np.asarray(net.link_type).copy()
+    st = np.asarray(net.init_status).copy()
+    vs = np.asarray(net.valve_setting_user, dtype=np.float64).copy()
+    kmi = np.asarray(net.km_int, dtype=np.float64).copy()
+    nt = np.asarray(net.node_type)
+    n1, n2 = np.asarray(net.link_n1).copy(), np.asarray(net.link_n2).copy()
+    el_m = np.asarray(net.elev_ft) * MperFT
+    hres = float(el_m[nt == RESERVOIR].max())
+    # nodes inside PRV zones: reachable from a PRV's downstream end without
+    # crossing another PRV
+    adj = [[] for _ in range(net.N)]
+    for k in range(net.L):
+        if lt[k] != PRV:
+            adj[n1[k]].append(n2[k])
+            adj[n2[k]].append(n1[k])
+    inzone = np.zeros(net.N, bool)
+    for k in np.flatnonzero(lt == PRV):
+        stack = [int(n2[k])]
+        while stack:
+            u = stack.pop()
+            if inzone[u]:
+                continue
+            inzone[u] = True
+            stack.extend(adj[u])
+    n_tree = net.N - 1
+    rng = np.random.default_rng(seed + 77)
+    cand = [k for k in range(n_tree) if lt[k] == PIPE and nt[n1[k]] == JUNCTION
+            and nt[n2[k]] == JUNCTION and not inzone[n1[k]] and not inzone[n2[k]]
+            and hres - el_m[n1[k]] > psv_margin_m + 20.0]
+    rng.shuffle(cand)
+    res0 = int(np.flatnonzero(nt == RESERVOIR)[0])
+
+    def reaches_all(skip):  # the network stays connected without link `skip`
+        nb = [[] for _ in range(net.N)]
+        for k in range(net.L):
+            if k != skip:
+                nb[n1[k]].append(n2[k])
+                nb[n2[k]].append(n1[k])
+        seen = np.zeros(net.N, bool)
+        stack = [res0]
+        while stack:
+            u = stack.pop()
+            if not seen[u]:
+                seen[u] = True
+                stack.extend(nb[u])
+        return bool(seen.all())
+
+    pick = (sorted(int(k) for k in psv_pick) if psv_pick is not None
+            else sorted([k for k in cand if reaches_all(k)][:psv_links]))
+    for i, k in enumerate(pick):
+        if psv_flip is not None and psv_flip[i]:
+            n1[k], n2[k] = n2[k], n1[k]
+        lt[k] = PSV
+        st[k] = 2
+        vs[k] = (hres - el_m[n1[k]] - psv_margin_m if psv_setting_m is None
+                 else float(psv_setting_m[i]))
+        d = float(net.diam_ft[k])
+        kmi[k] = 0.02517 * 0.5 / (d ** 2 * d ** 2)
+    f["link_type"] = lt.astype(np.int8)
+    f["init_status"] = st.astype(np.int8)
+    f["valve_setting_user"] = vs
+    f["km_int"] = kmi
+    f["link_n1"] = n1.astype(np.int32)
+    f["link_n2"] = n2.astype(np.int32)
+    return Net(**f)
