@@ -189,6 +189,12 @@ typedef struct WdsForwardOpts {
    * changed link k's status. */
   uint8_t* sched_flags;
   uint32_t* sched_chg;
+  /* Initial link statuses (WDS_XHEAD .. WDS_XPRESSURE), a device array
+   * int8 [B][L], or NULL for the network's status0: the status warm start
+   * of an extended-period step, which EpsDriver.run carries from frame to
+   * frame (run_gga(status0=S), dgga/eps.py:366-373).  Not with
+   * unroll_record. */
+  const int8_t* status0;
 } WdsForwardOpts;
 
 typedef struct WdsPlan WdsPlan;

@@ -618,9 +618,11 @@ class Model:
         return x
 
     def solve(self, d, rh, ke=None, r=None, accuracy=None, max_iter=None,
-              status_machine=False, q0=None, e0=None):
+              status_machine=False, q0=None, e0=None, S0=None):
         """Batched steady solve (restates solver.py:2703-3212); q0 [B or 1, L]
-        and e0 [B or 1, N] are the warm start of solver.py:2876-2887."""
+        and e0 [B or 1, N] are the warm start of solver.py:2876-2887; S0
+        [B or 1, L] the initial statuses (run_gga(status0=), the frame-to-frame
+        carry of dgga/eps.py:366-373)."""
         d = np.atleast_2d(np.asarray(d, dtype=np.float64))
         B = d.shape[0]
         rh = np.broadcast_to(np.atleast_2d(rh), (B, self.N))
@@ -650,7 +652,7 @@ class Model:
         maxtrials = max_iter
         S = nextcheck = None
         if sm:
-            S = np.broadcast_to(self.S0, (B, self.L)).copy()
+            S = np.broadcast_to(self.S0 if S0 is None else S0, (B, self.L)).copy()
             maxtrials = max_iter + (self.extra_iter if self.extra_iter > 0 else 0)
             nextcheck = np.full(B, self.checkfreq, dtype=np.int64)
         elif self.vmask.any() or self.is_cv.any():
@@ -925,7 +927,7 @@ class Model:
         return gd, grh, gke, gr
 
     def implicit(self, d, rh, ke=None, r=None, accuracy=1e-12, max_iter=200,
-                 polish_steps=3, status_machine=True, q0=None, e0=None):
+                 polish_steps=3, status_machine=True, q0=None, e0=None, S0=None):
         """Forward + polish; returns (out, state) where state feeds adjoint()."""
         d = np.atleast_2d(np.asarray(d, dtype=np.float64))
         B = d.shape[0]
@@ -934,7 +936,7 @@ class Model:
         r = self.r_hw if r is None else np.asarray(r, dtype=np.float64)
         r = np.broadcast_to(r, (B, self.L))
         out = self.solve(d, rh, ke=ke, r=r, accuracy=accuracy, max_iter=max_iter,
-                         status_machine=status_machine, q0=q0, e0=e0)
+                         status_machine=status_machine, q0=q0, e0=e0, S0=S0)
         if not out["converged"].all():
             raise RuntimeError("unconverged scenarios %s" %
                                np.flatnonzero(~out["converged"]).tolist())

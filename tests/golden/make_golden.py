@@ -18,6 +18,9 @@ and the reference outputs of
 
 Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
         python tests/golden/make_golden.py eps    (extended-period pin, eps_ref.npz)
+        python tests/golden/make_golden.py eps_events (small tanks that fill: shortened
+                                                   steps, tank links and a pump changing
+                                                   status, eps_events_ref.npz)
         python tests/golden/make_golden.py sens   (sensitivity-matrix pin, sens_ref.npz)
         python tests/golden/make_golden.py pumps  (pump-parameter gradient pins, pump_ref.npz
                                                    and chp_ref.npz)
@@ -205,12 +208,17 @@ def make_cfg3():
     write_cases(dgga, torch, cases)
 
 
-def make_eps(T=6):
+def make_eps(T=6, name="eps_ref", tank_range_m=10.0, tank_diam_m=(15.0, 30.0)):
     """Extended-period pin: the reference's serial EPANET-replica EpsDriver
-    (dgga/eps.py) on a small pump/tank network, one scenario, T hourly frames.
-    The scenario's noisy diurnal demands are given to the reference as one
-    demand pattern per junction.  Tank mid-range heads come from a reference
-    steady solve with the tank nodes as zero-demand junctions."""
+    (dgga/eps.py) on a small pump/tank network, one scenario, T hourly
+    demand periods (duration (T - 1) hours).  The scenario's noisy diurnal
+    demands are given to the reference as one demand pattern per junction.
+    Tank mid-range heads come from a reference steady solve with the tank
+    nodes as zero-demand junctions.  `eps` keeps the tanks inside their
+    range (hourly frames); `eps_events` uses small tanks (2 m range, 4-6 m
+    across) that fill within the run, so EpsDriver shortens steps at tank
+    fill/empty times, tank links close and reopen (tankstatus) and a pump
+    goes from XHEAD to open: eps_events_ref.npz."""
     import torch
     sys.path.insert(0, REPO)
     from wdsgpu_b200 import synth
@@ -236,7 +244,8 @@ def make_eps(T=6):
     o = pre.solve(torch.tensor(d0[None]), torch.tensor(np.nan_to_num(Net(**f).fixed_head_ft_at(0))[None]),
                   status_machine=True, accuracy=1e-8, assemble="csr", linear_solver="dense")
     centers = o["head_ft"][0].numpy()[tn]
-    net = synth.eps_network(seed=7, tank_center_ft=centers)
+    net = synth.eps_network(seed=7, tank_center_ft=centers, tank_range_m=tank_range_m,
+                            tank_diam_m=tank_diam_m)
     dem = synth.eps_demands(net, T, 1, seed=3)           # [T, 1, N] cfs
     # one pattern per junction reproduces dem[t, 0, node] = base * factor[t]
     fl = dict(net.as_fields())
@@ -255,10 +264,10 @@ def make_eps(T=6):
     blob.update({"in_demand": dem, "in_T": np.array(T)})
     for k in ("t_sec", "head_ft", "flow_int_cfs", "status", "iterations", "relerr"):
         blob["ref_" + k] = np.asarray(frames[k])
-    path = os.path.join(HERE, "eps_ref.npz")
+    path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **blob)
-    print("eps: frames at t=%s, iterations %s -> %s" % (
-        frames["t_sec"].tolist(), frames["iterations"].tolist(), os.path.basename(path)))
+    print("%s: frames at t=%s, iterations %s -> %s" % (
+        name, frames["t_sec"].tolist(), frames["iterations"].tolist(), os.path.basename(path)))
 
 
 def make_sens():
@@ -562,6 +571,8 @@ def make_unrolled():
 if __name__ == "__main__":
     if sys.argv[1:] == ["eps"]:
         make_eps()
+    elif sys.argv[1:] == ["eps_events"]:
+        make_eps(T=9, name="eps_events_ref", tank_range_m=2.0, tank_diam_m=(4.0, 6.0))
     elif sys.argv[1:] == ["sens"]:
         make_sens()
     elif sys.argv[1:] == ["pumps"]:

@@ -1,6 +1,7 @@
 """Extended-period oracle: pinned to the reference's EPANET-replica EpsDriver
-(fixture tests/golden/eps_ref.npz, made by `make_golden.py eps`), and its
-adjoint through time checked against central differences."""
+(fixtures tests/golden/eps_ref.npz and eps_events_ref.npz, made by
+`make_golden.py eps` / `eps_events`), and its adjoint through time checked
+against central differences."""
 import os
 import sys
 
@@ -15,62 +16,72 @@ from golden.load import load  # noqa: E402
 from oracle.eps import EpsOracle  # noqa: E402
 
 
-@pytest.fixture(scope="module")
-def case():
-    net, inp, ref = load("eps_ref")
-    return net, inp, ref
-
-
 def _rh(net, B):
     return np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), (B, net.N)).copy()
 
 
-def test_eps_oracle_matches_reference_eps_driver(case):
-    """Tank levels, junction heads and flows of every hourly frame agree with
-    dgga.eps.EpsDriver (which polishes nothing and stops at accuracy 1e-5;
-    the oracle's polished steps sit at the same fixed points)."""
-    net, inp, ref = case
-    T = int(inp["T"])
+@pytest.mark.parametrize("tag", ["eps_ref", "eps_events_ref"])
+def test_eps_oracle_matches_reference_eps_driver(tag):
+    """Frame times, tank levels, junction heads, flows and link statuses of
+    every frame agree with dgga.eps.EpsDriver (which polishes nothing and
+    stops at accuracy 1e-5; the oracle's polished frames sit at the same
+    fixed points).  In eps_events the tanks fill: EpsDriver shortens steps
+    at the fill times, tank links close and reopen, and a pump reopens from
+    XHEAD, all carried from frame to frame."""
+    net, inp, ref = load(tag)
     eo = EpsOracle(net)
-    run = eo.run(inp["demand"], _rh(net, 1), np.asarray(net.tank_h0)[None], accuracy=1e-9)
-    assert ref["t_sec"].tolist() == [3600 * t for t in range(T)]
+    runs = eo.run(inp["demand"], _rh(net, 1), np.asarray(net.tank_h0)[None], accuracy=1e-9)
+    fr = runs[0]
+    assert fr["t"] == ref["t_sec"].tolist()
     tn = np.asarray(net.tank_node)
     junc = np.asarray(net.node_type) == 0
-    assert np.abs(ref["head_ft"][:, tn] - run["tank_head"][:T, 0]).max() < 1e-7
-    assert np.abs(ref["head_ft"][:, junc] - run["head"][:, 0][:, junc]).max() < 1e-7
-    assert np.abs(ref["flow_int_cfs"] - run["flow"][:, 0]).max() < 1e-7
-    # the tanks do move (the pin is not vacuous)
-    assert np.abs(run["tank_head"][-1] - run["tank_head"][0]).max() > 0.05
+    head = np.stack(fr["head"])
+    assert np.abs(ref["head_ft"][:, tn] - np.stack(fr["tank_head"])).max() < 1e-7
+    assert np.abs(ref["head_ft"][:, junc] - head[:, junc]).max() < 1e-7
+    assert np.abs(ref["flow_int_cfs"] - np.stack(fr["flow"])).max() < 1e-7
+    np.testing.assert_array_equal(ref["status"], (np.stack(fr["status"]) > 2).astype(np.int8))
+    th = np.stack(fr["tank_head"])
+    assert np.abs(th[-1] - th[0]).max() > 0.05          # the tanks do move
+    if tag == "eps_events_ref":
+        assert any(t % 3600 for t in fr["t"])            # shortened steps
+        assert (np.diff(ref["status"], axis=0) != 0).any()  # statuses change
 
 
-def test_eps_oracle_adjoint_matches_central_difference(case):
-    net, inp, _ = case
-    T, B = 3, 2
+def test_eps_oracle_adjoint_matches_central_difference():
+    net, inp, _ = load("eps_ref")
+    P, B = 3, 2
     eo = EpsOracle(net)
     rng = np.random.default_rng(4)
-    dem = inp["demand"][:T, :1].repeat(B, 1) * rng.uniform(0.9, 1.1, (T, B, net.N))
+    dem = inp["demand"][:P, :1].repeat(B, 1) * rng.uniform(0.9, 1.1, (P, B, net.N))
     rh = _rh(net, B)
     th0 = np.broadcast_to(np.asarray(net.tank_h0), (B, len(net.tank_node))).copy()
     r = np.broadcast_to(np.asarray(net.r_hw), (B, net.L)).copy()
     sens = np.flatnonzero(np.asarray(net.node_type) == 0)[::7]
-    tn = np.asarray(net.tank_node)
     wq = rng.normal(size=net.L)
 
-    def loss_parts(run):
-        return ((run["head"][:, :, sens] ** 2).sum() + (run["tank_head"][-1] ** 2).sum()
-                + (run["flow"] * wq).sum())
+    def grads(runs):
+        gH = [[np.where(np.isin(np.arange(net.N), sens), 2.0 * h, 0.0) for h in fr["head"]]
+              for fr in runs]
+        gQ = [[wq for _ in fr["flow"]] for fr in runs]
+        gE = [[np.zeros(net.N) for _ in fr["flow"]] for fr in runs]
+        gT = [[np.zeros(len(net.tank_node)) for _ in fr["flow"]] for fr in runs]
+        for fr, g in zip(runs, gT):
+            g[-1] = 2.0 * fr["tank_head"][-1]
+        return gH, gQ, gE, gT
+
+    def loss_of(runs):
+        tot = 0.0
+        for fr in runs:
+            for h, q in zip(fr["head"], fr["flow"]):
+                tot += (h[sens] ** 2).sum() + (q * wq).sum()
+            tot += (fr["tank_head"][-1] ** 2).sum()
+        return tot
 
     def loss(d=dem, h0=th0, rr=r):
-        return loss_parts(eo.run(d, rh, h0, r=rr, accuracy=1e-12))
+        return loss_of(eo.run(d, rh, h0, r=rr, accuracy=1e-12))
 
-    run = eo.run(dem, rh, th0, r=r, accuracy=1e-12)
-    gH = np.zeros((T, B, net.N))
-    gH[:, :, sens] = 2.0 * run["head"][:, :, sens]
-    gQ = np.broadcast_to(wq, (T, B, net.L)).copy()
-    gE = np.zeros((T, B, net.N))
-    gT = np.zeros((T + 1, B, tn.size))
-    gT[T] = 2.0 * run["tank_head"][T]
-    g_dem, g_rh, g_h0, g_ke, g_r = eo.backward(run, gH, gQ, gE, gT)
+    runs = eo.run(dem, rh, th0, r=r, accuracy=1e-12)
+    g_dem, g_rh, g_h0, g_ke, g_r = eo.backward(runs, *grads(runs), P=P)
     checks = []
     j = int(sens[1])
     for (t, b) in ((0, 0), (2, 1)):

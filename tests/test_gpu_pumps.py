@@ -183,8 +183,11 @@ def test_clamp_branch_in_multi_and_eps_routes(cuda):
                     accuracy=1e-7)
     (out["head"] ** 2).sum().backward()
     eo = EpsOracle(net)
-    run = eo.run(dem, rh, th0, accuracy=1e-7)
-    g_dem = eo.backward(run, 2.0 * run["head"], np.zeros((T, B, net.L)),
-                        np.zeros((T, B, net.N)), np.zeros((T + 1, B, len(net.tank_node))))[0]
+    runs = eo.run(dem, rh, th0, accuracy=1e-7)
+    gH = [[2.0 * h for h in fr["head"]] for fr in runs]
+    gQ = [[np.zeros(net.L) for _ in fr["head"]] for fr in runs]
+    gE = [[np.zeros(net.N) for _ in fr["head"]] for fr in runs]
+    gT = [[np.zeros(len(net.tank_node)) for _ in fr["head"]] for fr in runs]
+    g_dem = eo.backward(runs, gH, gQ, gE, gT, P=T)[0]
     G = D.grad.cpu().numpy()
     assert np.abs(G - g_dem).max() <= 1e-7 * np.abs(g_dem).max()

@@ -68,7 +68,7 @@ class WdsForwardOpts(ctypes.Structure):
         ("pump_r", ctypes.c_void_p), ("pump_stride", ctypes.c_int64),
         ("refine_band", ctypes.c_double), ("unroll_record", ctypes.c_void_p),
         ("diag_ratio", ctypes.c_void_p), ("sched_flags", ctypes.c_void_p),
-        ("sched_chg", ctypes.c_void_p),
+        ("sched_chg", ctypes.c_void_p), ("status0", ctypes.c_void_p),
     ]
 
 

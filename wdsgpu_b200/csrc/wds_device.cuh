@@ -1306,7 +1306,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
   for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     s.q[k] = a.q0 ? a.q0[(size_t)b * n.L + k] : n.q_init[k];
-    s.S[k] = n.status0[k];
+    s.S[k] = a.s0 ? a.s0[(size_t)b * n.L + k] : n.status0[k];
   }
   gsync<NT>();
   const bool em_ok = build_emitters<NT>(n, s, kerow, 1);

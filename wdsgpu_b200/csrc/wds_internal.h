@@ -176,6 +176,7 @@ struct FwdArgs {
   double* diag;           // [B] diag_ratio, or null
   uint8_t* sflags;        // [B][maxtrials] schedule branch flags, or null
   uint32_t* schg;         // [B][maxtrials][ceil(L/32)] schedule change bits, or null
+  const int8_t* s0;       // [B][L] initial statuses, or null (the network's)
 };
 
 struct AdjArgs {

@@ -842,6 +842,9 @@ static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::
     return fail(WDS_E_ARG, who + ": sched_flags and sched_chg go together");
   if (a.sflags && !o->status_machine)
     return fail(WDS_E_ARG, who + ": the schedule record needs status_machine 1");
+  a.s0 = o->status0;
+  if (a.s0 && a.rec)
+    return fail(WDS_E_ARG, who + ": the unrolled mode starts from the network's statuses");
   if (a.rec && (o->status_machine || o->polish_steps >= 0))
     return fail(WDS_E_ARG, who + ": the unrolled mode runs with status_machine 0 and no polish");
   a.th_sp = o->pump_speed;

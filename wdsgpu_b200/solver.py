@@ -633,7 +633,7 @@ class GGASolver:
 
     def run(self, d, rh, ke, r, B, max_iter, hacc, status_machine, polish_steps,
             refine=None, plan=None, q0=None, e0=None, pumps=None, refine_band=None,
-            record=None, schedule=False):
+            record=None, schedule=False, S0=None):
         """One wds_forward call on device tensors; returns the raw outputs.
         q0 [B,L] / e0 [B,N] (contiguous FP64 on the device, or None) are the
         warm start of GGASolver.solve (dgga/solver.py:2876-2887); pumps is
@@ -671,6 +671,10 @@ class GGASolver:
         o.polish_steps = int(polish_steps)
         o.ke_stride = 0 if ke.shape[0] == 1 else self.N
         o.r_stride = 0 if r.shape[0] == 1 else self.L
+        if S0 is not None:       # status warm start (extended-period steps)
+            if S0.dtype != torch.int8 or not S0.is_contiguous() or tuple(S0.shape) != (B, self.L):
+                raise ValueError("S0 must be a contiguous int8 [%d, %d] tensor" % (B, self.L))
+            o.status0 = S0.data_ptr()
         for name, t, cols in (("q0", q0, self.L), ("e0", e0, self.N)):
             if t is not None:
                 same_dev = t.device.type == dev.type and (dev.index is None
