@@ -575,11 +575,11 @@ __device__ __forceinline__ void fwd_range(const TB& T, const FT* W, double* v, i
   }
 }
 
-// One backward-substitution level: x_j = u_j - (1/D_j) sum_i L_ij D_j x_i.
+// One backward-substitution level, columns [c0, c1):
+// x_j = u_j - (1/D_j) sum_i L_ij D_j x_i.
 template <class TB, class FT>
-__device__ __forceinline__ void bwd_level(const TB& T, const FT* W, double* v, int lv,
+__device__ __forceinline__ void bwd_level(const TB& T, const FT* W, double* v, int c0, int c1,
                                           int lg, int t, int nthr) {
-  const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
   const int G = 1 << lg, li = t & (G - 1), per = nthr >> lg;
   for (int base = c0; base < c1; base += per) {
     const int j = base + (t >> lg);
@@ -737,10 +737,17 @@ __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
   bool bad = false, prev_wide = true;
+  // a level's mode and slot range are static: the next level's are loaded
+  // while this level runs, so that a level starts with its own work
+  int md_n = n.L0 > 0 ? T.mfac[0] : 0, t1_n = n.L0 > 0 ? T.colptr[T.levptr[1]] : 0;
+  int t0 = 0;
   for (int lv = 0; lv < n.L0; ++lv) {
-    const int md = T.mfac[lv];
+    const int md = md_n, t1 = t1_n;
+    if (lv + 1 < n.L0) {
+      md_n = T.mfac[lv + 1];
+      t1_n = T.colptr[T.levptr[lv + 2]];
+    }
     const bool wide = (md & 0x80) != 0;
-    const int t0 = T.colptr[T.levptr[lv]], t1 = T.colptr[T.levptr[lv + 1]];
     if (wide) {
       if (!prev_wide) gsync<NT>();
       fac_range(T, wp<FT>(s), t0, t1, md & 7, tid, NT, bad);
@@ -750,6 +757,7 @@ __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
       __syncwarp();
     }
     prev_wide = wide;
+    t0 = t1;
   }
   if (n.nT > 0) {
     // Schur complement of the top block: its slots minus the lower columns' updates
@@ -771,10 +779,16 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
   const int tid = gtid<NT>(), lane = tid & 31;
   const bool inw = tid < 32;
   bool prev_wide = true;
+  // each level's mode and column range come from registers loaded a level ahead
+  int md_n = n.L0 > 0 ? T.mfwd[0] : 0, c1_n = n.L0 > 0 ? T.levptr[1] : 0;
+  int c0 = 0;
   for (int lv = 0; lv < n.L0; ++lv) {
-    const int md = T.mfwd[lv];
+    const int md = md_n, c1 = c1_n;
+    if (lv + 1 < n.L0) {
+      md_n = T.mfwd[lv + 1];
+      c1_n = T.levptr[lv + 2];
+    }
     const bool wide = (md & 0x80) != 0;
-    const int c0 = T.levptr[lv], c1 = T.levptr[lv + 1];
     if (wide) {
       if (!prev_wide) gsync<NT>();
       fwd_range(T, (const FT*)wp<FT>(s), v, c0, c1, md & 7, tid, NT, false);
@@ -784,6 +798,7 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
       __syncwarp();
     }
     prev_wide = wide;
+    c0 = c1;
   }
   if (n.nT > 0) {
     const int md = T.mfwd[n.L0];
@@ -794,18 +809,25 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
     top_apply<NT>(s.Mg, v + n.cT, n.nT);
     prev_wide = true;
   }
+  int mb_n = n.L0 > 0 ? T.mbwd[n.L0 - 1] : 0, b0_n = n.L0 > 0 ? T.levptr[n.L0 - 1] : 0;
+  int b1 = n.L0 > 0 ? T.levptr[n.L0] : 0;
   for (int lv = n.L0 - 1; lv >= 0; --lv) {
-    const int md = T.mbwd[lv];
+    const int md = mb_n, b0 = b0_n;
+    if (lv > 0) {
+      mb_n = T.mbwd[lv - 1];
+      b0_n = T.levptr[lv - 1];
+    }
     const bool wide = (md & 0x80) != 0;
     if (wide) {
       if (!prev_wide) gsync<NT>();
-      bwd_level(T, (const FT*)wp<FT>(s), v, lv, md & 7, tid, NT);
+      bwd_level(T, (const FT*)wp<FT>(s), v, b0, b1, md & 7, tid, NT);
       gsync<NT>();
     } else if (inw) {
-      bwd_level(T, (const FT*)wp<FT>(s), v, lv, md & 7, lane, 32);
+      bwd_level(T, (const FT*)wp<FT>(s), v, b0, b1, md & 7, lane, 32);
       __syncwarp();
     }
     prev_wide = wide;
+    b1 = b0;
   }
   gsync<NT>();
 }
@@ -870,7 +892,31 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
   for (int p = tid; p < n.Nj; p += NT) {
     const int a = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
     double dg = 0.0, xf = 0.0, F = 0.0;
-    for (int e = a; e < m; ++e) {
+    // the link flows and Y live in L2: the first kPre incident links' values
+    // are requested together, then summed in the reference's order (n1 side,
+    // then n2 side); a junction with more links loads the rest one by one
+    constexpr int kPre = 4;
+    double qv[kPre], yv[kPre];
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      qv[u] = yv[u] = 0.0;
+      if (a + u < z) {
+        const int k = T.inc[a + u] & 0xffff;
+        qv[u] = s.q[k];
+        yv[u] = s.Y[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int e = a + u;
+      if (e >= m) break;
+      const uint32_t ie = T.inc[e];
+      if (ie & (1u << 16)) continue;
+      dg += s.P[ie & 0xffff];
+      xf += -qv[u];
+      F += yv[u];
+    }
+    for (int e = a + kPre; e < m; ++e) {
       const uint32_t ie = T.inc[e];
       if (ie & (1u << 16)) continue;
       const int k = ie & 0xffff;
@@ -878,7 +924,17 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       xf += -s.q[k];
       F += s.Y[k];
     }
-    for (int e = m; e < z; ++e) {
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int e = a + u;
+      if (e < m || e >= z) continue;
+      const uint32_t ie = T.inc[e];
+      if (ie & (1u << 16)) continue;
+      dg += s.P[ie & 0xffff];
+      xf += qv[u];
+      F += -yv[u];
+    }
+    for (int e = (m > a + kPre ? m : a + kPre); e < z; ++e) {
       const uint32_t ie = T.inc[e];
       if (ie & (1u << 16)) continue;
       const int k = ie & 0xffff;
@@ -1332,12 +1388,23 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       for (int p = gtid<NT>(); p < n.Nj; p += NT)
         r[n.L + p] = s.eslot[p] >= 0 ? s.em_e[s.eslot[p]] : 0.0;
     }
-    // ---- headloss coefficients
-    for (int k = gtid<NT>(); k < n.L; k += NT) {
-      double P, Y;
-      link_coef(n, th, k, s.q[k], s.S[k], rrow[k], false, P, Y);
-      s.P[k] = P;
-      s.Y[k] = Y;
+    // ---- headloss coefficients (the next link's flow and resistance, in L2,
+    // are loaded while this link's coefficients are formed)
+    {
+      int k = gtid<NT>();
+      double qn = k < n.L ? s.q[k] : 0.0, rn = k < n.L ? rrow[k] : 0.0;
+      for (; k < n.L; k += NT) {
+        const double qk = qn, rk = rn;
+        const int kn = k + NT;
+        if (kn < n.L) {
+          qn = s.q[kn];
+          rn = rrow[kn];
+        }
+        double P, Y;
+        link_coef(n, th, k, qk, s.S[k], rk, false, P, Y);
+        s.P[k] = P;
+        s.Y[k] = Y;
+      }
     }
     gsync<NT>();
     assemble_gga<NT, FT>(n, T, s, kerow, drow);
@@ -1366,14 +1433,24 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     }
     // ---- newflows (hydsolver.c:358-514 as restated in solver.py:3092-3110)
     double sums[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = gtid<NT>(); k < n.L; k += NT) {
-      const double dh = head_of(T.e1[k], s.V1, s.hf) - head_of(T.e2[k], s.V1, s.hf);
-      double dq = s.Y[k] - s.P[k] * dh;
-      if ((n.flags[k] & WDS_F_CHP) && dq > s.q[k]) dq = s.q[k] / 2.0;
-      const double qn = s.q[k] - dq;
-      s.q[k] = qn;
-      sums[0] += fabs(dq);
-      sums[1] += fabs(qn);
+    {
+      int k = gtid<NT>();
+      double yn = k < n.L ? s.Y[k] : 0.0, qn = k < n.L ? s.q[k] : 0.0;  // next link's, from L2
+      for (; k < n.L; k += NT) {
+        const double yk = yn, qk = qn;
+        const int kn = k + NT;
+        if (kn < n.L) {
+          yn = s.Y[kn];
+          qn = s.q[kn];
+        }
+        const double dh = head_of(T.e1[k], s.V1, s.hf) - head_of(T.e2[k], s.V1, s.hf);
+        double dq = yk - s.P[k] * dh;
+        if ((n.flags[k] & WDS_F_CHP) && dq > qk) dq = qk / 2.0;
+        const double q2 = qk - dq;
+        s.q[k] = q2;
+        sums[0] += fabs(dq);
+        sums[1] += fabs(q2);
+      }
     }
     for (int p = gtid<NT>(); p < n.Nj; p += NT) {
       const int es = s.eslot[p];
