@@ -359,6 +359,41 @@ def run_reference_code(args):
     print(json.dumps(line), flush=True)
 
 
+def run_tune(args):
+    """`--workload tune`: the measured autotuner (wdsgpu_b200.tune) on the
+    four networks of the mixed-size workload, each at `--batch` scenarios
+    (default 256): the cost model's forward + adjoint step time beside the
+    tuned one, and the choice.  One JSON line."""
+    import tempfile
+    import torch
+    from wdsgpu_b200 import synth, tune
+    from wdsgpu_b200.solver import GGASolver
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    B = 256 if args.batch == 1024 else args.batch
+    names = ("100 jn / 120 pipes", "542 jn / 554 links, 79 TCVs", "782 jn / 905 pipes / 3 PRVs",
+             "3000 jn / 3600 pipes")
+    cache = os.path.join(tempfile.mkdtemp(), "tune.json")
+    res = {}
+    with ClockSampler(None) as clk:
+        for name, net in zip(names, synth.config3_networks()):
+            s = GGASolver(net, device=dev, dense_status_machine=True)
+            r = tune.autotune(s, B, repeats=max(3, args.steps), cache_path=cache)
+            res[name] = {"model_ms": r["model_ms"], "tuned_ms": r["ms"], "choice": r["choice"],
+                         "candidates": len(r["tried"])}
+    tot_m = sum(v["model_ms"] for v in res.values())
+    tot_t = sum(v["tuned_ms"] for v in res.values())
+    line = {"metric": "autotuned fwd+adjoint step time over the mixed-size networks "
+                      "(sum of the four, B=%d each)" % B,
+            "value": tot_t, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": tot_t, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config-3 networks, one solver each, B=%d lognormal(0.2) "
+                                   "scenarios; median of the timed steps per candidate" % B},
+            "cost_model_ms": tot_m, "networks": res, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ secondary workloads
 def run_secondary(args):
     """Mixed-size one-launch, extended-period and unrolled-K workloads: one JSON line."""
@@ -539,12 +574,16 @@ def main():
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="config2",
-                    choices=("config2", "config4", "mixed", "eps", "unrolled", "refgpu", "refcpu"))
+                    choices=("config2", "config4", "mixed", "eps", "unrolled", "refgpu", "refcpu",
+                             "tune"))
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload in ("refgpu", "refcpu"):
         run_reference_code(args)
+        return
+    if args.workload == "tune":
+        run_tune(args)
         return
     if args.workload == "config4":
         args.batch = 16384 if args.batch == 1024 else args.batch

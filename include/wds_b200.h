@@ -124,6 +124,14 @@ typedef struct WdsNetwork {
   const double* pump_hunit;      /* [L] pumpstatus shut-off head at unit speed (BIG for
                                     constant-HP pumps), used when a call passes its own
                                     pump speeds; NULL: pump_hmax / pump_speed^2 */
+  /* Schedule choices the planner otherwise takes from its cost model (no
+   * counterpart in the reference; set by the autotuner,
+   * wdsgpu_b200/tune.py).  Each 0 means the planner's choice.  They change
+   * the schedule, not the algorithm: results agree within rounding. */
+  int32_t groups_per_cta;        /* scenario groups of 256 threads per CTA, 1-4 */
+  int32_t top_max;               /* most columns of the dense top block (1-48), -1: none */
+  double level_barrier_cost;     /* cost of a group barrier in the per-level mode model
+                                    (in dependent rounds; 0: 0.5) */
 } WdsNetwork;
 
 /* WdsNetwork.layout */

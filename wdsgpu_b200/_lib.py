@@ -55,6 +55,8 @@ class WdsNetwork(ctypes.Structure):
         ("emitter_capacity", ctypes.c_int32),
         ("layout", ctypes.c_int32), ("factor_fp32", ctypes.c_int32),
         ("pump_hunit", c_double_p),
+        ("groups_per_cta", ctypes.c_int32), ("top_max", ctypes.c_int32),
+        ("level_barrier_cost", ctypes.c_double),
     ]
 
 

@@ -263,9 +263,14 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   // complement S (updates from the columns below only) is inverted densely,
   // and each substitution applies S^{-1} in one step instead of one step per
   // level in each sweep.  Worth it from three top levels on.
+  if (net->top_max < -1 || net->top_max > WDS_TOP_MAX || net->groups_per_cta < 0 ||
+      net->groups_per_cta > 4 || !(net->level_barrier_cost >= 0.0))
+    return fail(WDS_E_ARG, "wds_plan: top_max must be -1..48, groups_per_cta 0..4, "
+                           "level_barrier_cost >= 0");
+  const int top_cap = net->top_max > 0 ? net->top_max : WDS_TOP_MAX;
   int L0 = nlev;
-  for (int l = nlev - 1; l >= 0 && Nj - levptr[l] <= WDS_TOP_MAX; --l) L0 = l;
-  if (nlev - L0 < 3) L0 = nlev;
+  for (int l = nlev - 1; l >= 0 && Nj - levptr[l] <= top_cap; --l) L0 = l;
+  if (nlev - L0 < 3 || net->top_max < 0) L0 = nlev;
   const int cT = levptr[L0], nT = Nj - cT;
   auto slot = [&](int i, int j) -> int {  // slot of L_ij, i >= j; -1 if structurally zero
     if (i == j) return colptr[j];
@@ -320,14 +325,16 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
   // followed by a group barrier) instead of narrow (warp 0 only, __syncwarp).
   // Cost model in units of one dependent round: rounds * (ceil(maxlen / G) +
   // 0.6 log2 G + 1), plus 0.5 per group barrier.
-  auto pick_mode = [](int count, int maxlen) -> uint8_t {
+  const double bar_cost = net->level_barrier_cost > 0.0 ? net->level_barrier_cost : 0.5;
+  auto pick_mode = [bar_cost](int count, int maxlen) -> uint8_t {
     double best = 1e30;
     uint8_t mode = 0;
     for (int wide = 0; wide <= 1; ++wide)
       for (int lg = 0; lg <= 5; ++lg) {
         const int G = 1 << lg, per = (wide ? 256 : 32) / G;
         const double rounds = (double)((count + per - 1) / per);
-        const double cost = rounds * ((maxlen + G - 1) / G + 0.6 * lg + 1.0) + (wide ? 0.5 : 0.0);
+        const double cost =
+            rounds * ((maxlen + G - 1) / G + 0.6 * lg + 1.0) + (wide ? bar_cost : 0.0);
         if (cost < best - 1e-12) { best = cost; mode = (uint8_t)(lg | (wide ? 0x80 : 0)); }
       }
     return mode;
@@ -767,6 +774,15 @@ extern "C" int wds_plan(const WdsNetwork* net, int32_t max_batch, WdsPlan** out)
       int ctas = (int)((228 * 1024) / (sm + 1024));
       ctas = std::min(ctas, 2048 / (256 * g));
       if (ctas * g > best_res) { best_res = ctas * g; best_g = g; }
+    }
+    if (net->groups_per_cta > 0) {  // a tuned choice, if the state fits
+      if ((size_t)d.stab_bytes + net->groups_per_cta * st > 227 * 1024) {
+        cudaFree(plan->dtab);
+        delete plan;
+        return fail(WDS_E_ARG, "wds_plan: groups_per_cta " + std::to_string(net->groups_per_cta) +
+                                   " exceeds shared memory for this network");
+      }
+      best_g = net->groups_per_cta;
     }
     plan->groups = best_g;
     plan->smem_fwd = best_g ? (size_t)d.stab_bytes + best_g * st : (size_t)d.stab_bytes + st;

@@ -79,6 +79,10 @@ class _Plan:
         if solver.sm100_factor_dtype not in (torch.float64, torch.float32):
             raise ValueError("sm100_factor_dtype must be torch.float64 or torch.float32")
         net.factor_fp32 = 1 if solver.sm100_factor_dtype == torch.float32 else 0
+        tun = solver.sm100_tuning or {}
+        net.groups_per_cta = int(tun.get("groups_per_cta", 0))
+        net.top_max = int(tun.get("top_max", 0))
+        net.level_barrier_cost = float(tun.get("level_barrier_cost", 0.0))
         with torch.cuda.device(self.device):
             _lib.check(lib.wds_plan(ctypes.byref(net), self.max_batch,
                                     ctypes.byref(self.handle)), "wds_plan")
@@ -235,6 +239,9 @@ class GGASolver:
         self.sm100_refine = 2
         self.sm100_refine_band = None
         self.sm100_layout = "auto"
+        # schedule choices of the planner (groups_per_cta, top_max,
+        # level_barrier_cost; None: its cost model), set by wdsgpu_b200.tune
+        self.sm100_tuning = None
         self.sm100_factor_dtype = torch.float64
         # emitters per scenario kept in shared memory (junctions with Ke > 0)
         self.emitter_capacity = max(64, 2 * int((np.asarray(net.node_ke) > 0).sum()))
