@@ -343,7 +343,7 @@ int wds_adjoint_multi(int32_t nplans, WdsPlan* const* plans, const int32_t* batc
  * per-scenario workspace lives in one fixed WDS_NOALLOC_SCRATCH_BYTES device
  * array held by every GPU that loads the library until the process exits,
  * so the call never calls cudaMalloc or cudaFree.  A batch whose workspace
- * exceeds the array (about 400 scenarios of a 782-junction network) is
+ * exceeds the array (about 340 scenarios of a 782-junction network) is
  * rejected with WDS_E_ARG.  The first call on a device loads the library's
  * device code there, which creates the array; make that first call before
  * any stream capture.  Calls share the array and it keeps the last call's

@@ -887,10 +887,13 @@ __device__ void dense_solve(double* C, double* y, int m) {
 // into W (pattern of L) and F = V0; Xflow saved for PRV downstream nodes.
 template <int NT, class FT, class TB>
 __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const double* kerow,
-                             const double* drow) {
+                             const double* dj) {
   const int tid = gtid<NT>();
   for (int p = tid; p < n.Nj; p += NT) {
     const int a = T.inc_ptr[p], m = T.inc_split[p], z = T.inc_ptr[p + 1];
+    // the junction's global values are requested before its incidence sums
+    const double dem = dj[p];
+    const int xfs = n.node_xf[p];
     double dg = 0.0, xf = 0.0, F = 0.0;
     // the link flows and Y live in L2: the first kPre incident links' values
     // are requested together, then summed in the reference's order (n1 side,
@@ -952,7 +955,6 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       if ((ie & (1u << 16)) || !(ie & (1u << 17))) continue;
       F += s.P[ie & 0xffff] * s.hf[ie >> 18];
     }
-    const int nd = n.jnode[p];
     const int es = s.eslot[p];
     if (es >= 0) {
       double hl, hg;
@@ -963,11 +965,11 @@ __device__ void assemble_gga(const DevNet& n, const TB& T, const Sh& s, const do
       F = F + (hl + n.el[p]) / hg;
       xf = xf - s.em_e[es];
     }
-    xf = xf - drow[nd];
+    xf = xf - dem;
     F = F + xf;
     wp<FT>(s)[T.colptr[p]] = (FT)dg;
     s.V0[p] = F;
-    if (n.node_xf[p] >= 0) s.xf[n.node_xf[p]] = xf;
+    if (xfs >= 0) s.xf[xfs] = xf;
   }
   for (int t = tid; t < n.npairs; t += NT) {
     double v = 0.0;
@@ -1359,6 +1361,10 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
   const double* drow = a.d + (long long)b * n.N;
   const double* rhrow = a.rh + (long long)b * n.N;
   const PumpTh th = pump_th(n, a, b);
+  // the scenario's junction demands in elimination order, gathered once and
+  // read coalesced by every assembly
+  double* dj = w.dj + (size_t)b * n.Nj;
+  for (int p = gtid<NT>(); p < n.Nj; p += NT) dj[p] = drow[n.jnode[p]];
   for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     s.q[k] = a.q0 ? a.q0[(size_t)b * n.L + k] : n.q_init[k];
@@ -1407,7 +1413,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       }
     }
     gsync<NT>();
-    assemble_gga<NT, FT>(n, T, s, kerow, drow);
+    assemble_gga<NT, FT>(n, T, s, kerow, dj);
     if (a.diag && n.npcv > 0) {  // condition proxy (dgga/solver.py:3026-3032)
       double mx = 0.0, mn = kINF;
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
@@ -1644,7 +1650,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
           mm = mm - s.em_e[es];
           emh = s.em_emh[es];
         }
-        mm = mm - drow[n.jnode[p]];
+        mm = mm - dj[p];
         s.V0[p] = (mm - bt) + emh * re;
       }
       gsync<NT>();
@@ -2076,6 +2082,8 @@ __device__ __forceinline__ void unrolled_one(const DevNet& n, const DevWork& w, 
   const double* rhrow = u.rh + (size_t)b * n.N;
   FwdArgs a0{};  // the network's own pump parameters
   const PumpTh th = pump_th(n, a0, b);
+  double* dj = w.dj + (size_t)b * n.Nj;  // junction demands in elimination order
+  for (int p = tid; p < n.Nj; p += NT) dj[p] = drow[n.jnode[p]];
   for (int f = tid; f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
   for (int k = tid; k < n.L; k += NT) s.S[k] = n.status0[k];
   gsync<NT>();
@@ -2120,7 +2128,7 @@ __device__ __forceinline__ void unrolled_one(const DevNet& n, const DevWork& w, 
       s.Y[k] = Y;
     }
     gsync<NT>();
-    assemble_gga<NT, FT>(n, T, s, kerow, drow);
+    assemble_gga<NT, FT>(n, T, s, kerow, dj);
     factor<NT, FT>(n, T, s);  // the forward factored this matrix: positive definite
     // (1) q' = q - dq: the head-difference adjoint of each link
     for (int k = tid; k < n.L; k += NT) {

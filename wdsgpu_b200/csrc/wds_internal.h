@@ -144,6 +144,7 @@ struct DevWork {
   double* M;      // [B][nT][nT] inverse of the top block's Schur complement
   unsigned char* state;  // [B][state bytes] scenario state of large networks (else null)
   double* dpump;  // [B][3][npump] dhloss/d(speed, H0, R) of each pump at the terminal state
+  double* dj;     // [B][Nj] the scenario's junction demands in elimination order
   int nscr;
   int* valid;     // [B] 1 when the terminal state is stored
 };

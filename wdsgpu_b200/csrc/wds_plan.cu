@@ -85,7 +85,7 @@ struct Blob {
 // 256-byte aligned.  One function for the plan's own workspace and for the
 // fixed array of wds_forward_noalloc, so the two layouts cannot drift apart.
 struct WorkOff {
-  size_t W, P, dr, emh, hge, dke, act, scr, valid, lk, M, state, pump, bytes;
+  size_t W, P, dr, emh, hge, dke, act, scr, valid, lk, M, state, pump, dj, bytes;
 };
 
 WorkOff work_layout(const wds::DevNet& d, int nscr, size_t B, size_t state_bytes) {
@@ -98,6 +98,7 @@ WorkOff work_layout(const wds::DevNet& d, int nscr, size_t B, size_t state_bytes
   o.act = take(B * pc); o.scr = take(B * (size_t)nscr * d.Nj * 8); o.valid = take(B * 4);
   o.lk = take(B * 2 * d.L * 8); o.M = take(B * (size_t)std::max(d.nT * d.nT, 1) * 8);
   o.state = take(d.wide ? B * state_bytes : 0); o.pump = take(B * 3 * (size_t)d.npump * 8);
+  o.dj = take(B * d.Nj * 8);
   o.bytes = bytes;
   return o;
 }
@@ -112,6 +113,7 @@ wds::DevWork work_at(unsigned char* base, const WorkOff& o, const wds::DevNet& d
   w.lk = (double*)(base + o.lk); w.M = (double*)(base + o.M);
   w.state = d.wide ? base + o.state : nullptr;
   w.dpump = (double*)(base + o.pump);
+  w.dj = (double*)(base + o.dj);
   w.nscr = nscr;
   return w;
 }
