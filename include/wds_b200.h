@@ -176,7 +176,8 @@ typedef struct WdsForwardOpts {
   /* Unrolled-K mode (solve_unrolled, dgga/autodiff.py:1357-1664): a device
    * array [B][max_iter][L + 2 Nj] or NULL.  When set, the call runs exactly
    * max_iter GGA iterations with no convergence test (status_machine must be
-   * 0 and polish_steps < 0, the statuses stay the initial ones) and records
+   * 0 and polish_steps < 0, the statuses stay frozen: status0 or the
+   * network's initial ones; q0 / e0 give the starting flows) and records
    * each iteration's starting flows, emitter flows (by junction) and
    * solved junction heads there, for wds_unrolled_adjoint. */
   double* unroll_record;
@@ -252,7 +253,9 @@ int wds_adjoint_pumps(WdsPlan* plan, int32_t batch, const double* gH,
  * the K iterations maps the output adjoints gH [B,N], gQ [B,L], gE [B,N] to
  * gd, grh, gke [B,N] and gr [B,L] (per scenario; a shared parameter takes
  * the batch sum).  demand / fixed_head / ke / r are the forward's inputs.
- * scratch: device array [B][2 L + 2 Nj].  Networks with control valves
+ * scratch: device array [B][2 L + 2 Nj]; status0: the frozen statuses the
+ * forward ran with (its opts.status0, the `status` of solve_unrolled) or
+ * NULL for the network's.  Networks with control valves
  * (PRV/PSV/FCV with a setting) are refused, as by the reference.  Rebuilds
  * each iteration's factor in the plan's workspace, so a kept implicit state
  * is gone afterwards. */
@@ -260,7 +263,8 @@ int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K, const double* 
                          const double* demand, const double* fixed_head, const double* ke,
                          int64_t ke_stride, const double* r, int64_t r_stride,
                          const double* gH, const double* gQ, const double* gE, double* gd,
-                         double* grh, double* gke, double* gr, double* scratch, void* stream);
+                         double* grh, double* gke, double* gr, double* scratch,
+                         const int8_t* status0, void* stream);
 
 /* Statistics of the plan: [Nj, nnz_L, n_levels, n_pairs, smem_bytes,
  * n_pcv, nnz_A_lower, threads]. */

@@ -161,8 +161,10 @@ class Unrolled:
         return hle, hge, hle_e, hge_e, hle_k, hge_k
 
     # ---------------------------------------------------------------- forward
-    def forward(self, d, rh, ke=None, r=None, K=8, S=None):
-        """K iterations from the initial flows (emitter flows 1); returns the
+    def forward(self, d, rh, ke=None, r=None, K=8, S=None, q0=None, e0=None):
+        """K iterations from the initial flows (emitter flows 1), or from the
+        warm start q0 [B or 1, L] / e0 [B or 1, N] of solve_unrolled
+        (dgga/autodiff.py:1357-1360), with the statuses S frozen; returns the
         outputs and the record the reverse pass reads."""
         m = self.m
         d = np.atleast_2d(np.asarray(d, dtype=np.float64))
@@ -175,8 +177,13 @@ class Unrolled:
         S = np.broadcast_to(m.S0 if S is None else np.asarray(S, dtype=np.int8), (B, m.L)).copy()
         ke_j, d_j = ke[:, m.junc], d[:, m.junc]
         em = (ke_j > 0.0).astype(float)
-        q = np.broadcast_to(m.init_flow(), (B, m.L)).copy()
-        e = em.copy()
+        q = np.broadcast_to(m.init_flow() if q0 is None else np.asarray(q0, dtype=np.float64),
+                            (B, m.L)).copy()
+        if e0 is None:
+            e = em.copy()
+        else:
+            e0 = np.broadcast_to(np.atleast_2d(np.asarray(e0, dtype=np.float64)), (B, m.N))
+            e = np.where(em > 0, e0[:, m.junc], 0.0)
         H = np.zeros((B, m.N))
         H[:, m.fixed] = rh[:, m.fixed]
         rec = []

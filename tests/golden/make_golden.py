@@ -27,6 +27,8 @@ Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
         python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
         python tests/golden/make_golden.py unrolled (unrolled-K gradient pin, unrolled_ref.npz)
+        python tests/golden/make_golden.py unrolled_warm (warm start and frozen statuses,
+                                                   unrolled_warm_ref.npz)
         python tests/golden/make_golden.py valves (8 PRVs + 2 PSVs on one network, valves_ref.npz)
         python tests/golden/make_golden.py contract (diag_ratio and record_schedule of solve(),
                                                    contract_ref.npz)
@@ -568,6 +570,54 @@ def make_unrolled():
                                                          os.path.basename(path)))
 
 
+def make_unrolled_warm():
+    """Unrolled-K pin with a warm start and frozen statuses: the reference's
+    solve_unrolled (dgga/autodiff.py:1357-1664) at K = 6 from the flows and
+    emitter flows of its own dense solve at 90 % demand (q0 [B,L], e0 [B,N])
+    and with the statuses that solve ended with frozen (status [L]), on the
+    unrolled feature network."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.unrolled_network()
+    d, _ = synth.config2_scenarios(net, 3, seed=43, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    ke = np.broadcast_to(np.asarray(net.node_ke, dtype=np.float64), d.shape).copy()
+    sens = synth.sensor_nodes(net, 6)
+    pl = np.asarray(net.pump_link, dtype=np.int64)
+    emn = np.flatnonzero(np.asarray(net.node_ke) > 0)
+    K = 6
+    ref_net = dgga.parse.Net(**net.as_fields())
+    sd = dgga.solver.GGASolver(ref_net, device="cpu", mode="dense", dense_status_machine=True)
+    f = sd.solve(torch.tensor(0.9 * d), torch.tensor(rh), ke_int=torch.tensor(ke),
+                 status_machine=True, accuracy=1e-6, assemble="csr", linear_solver="dense")
+    q0 = f["flow_cfs"].numpy()
+    e0 = f["emitter_cfs"].numpy()
+    st = f["status"].numpy()[0].astype(np.int8)
+    D = torch.tensor(d).requires_grad_(True)
+    RH = torch.tensor(rh).requires_grad_(True)
+    KE = torch.tensor(ke).requires_grad_(True)
+    R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64)).requires_grad_(True)
+    out = dgga.autodiff.solve_unrolled(sd, D, RH, ke=KE, r_hw=R, K=K, q0=torch.tensor(q0),
+                                       e0=torch.tensor(e0), status=st)
+    h, q, e = out["head_ft"], out["flow_cfs"], out["emitter_cfs"]
+    loss = (h[:, sens] ** 2).sum() + (q[:, pl] ** 2).sum() + (e[:, emn] ** 2).sum()
+    loss.backward()
+    blob = pack_net(net)
+    blob.update({"in_demand": d, "in_res_head": rh, "in_ke": ke, "in_sensors": np.asarray(sens),
+                 "in_K": np.array(K), "in_q0": q0, "in_e0": e0, "in_status": st})
+    res = dict(head=h.detach().numpy(), flow=q.detach().numpy(), emitter=e.detach().numpy(),
+               g_demand=D.grad.numpy(), g_res_head=RH.grad.numpy(), g_ke=KE.grad.numpy(),
+               g_rhw=R.grad.numpy())
+    blob.update({"ref_" + k: v for k, v in res.items()})
+    path = os.path.join(HERE, "unrolled_warm_ref.npz")
+    np.savez_compressed(path, **blob)
+    print("unrolled_warm: K=%d, statuses %s -> %s" % (K, np.bincount(st).tolist(),
+                                                      os.path.basename(path)))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["eps"]:
         make_eps()
@@ -583,6 +633,8 @@ if __name__ == "__main__":
         make_psv()
     elif sys.argv[1:] == ["unrolled"]:
         make_unrolled()
+    elif sys.argv[1:] == ["unrolled_warm"]:
+        make_unrolled_warm()
     elif sys.argv[1:] == ["cfg3"]:
         make_cfg3()
     elif sys.argv[1:] == ["valves"]:

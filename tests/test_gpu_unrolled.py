@@ -1,8 +1,9 @@
 """Unrolled-K differentiation on the B200 route (solve_unrolled): the
 recording forward and wds_unrolled_adjoint against the reference's
 solve_unrolled and its autograd gradients (fixture
-tests/golden/unrolled_ref.npz) and against the oracle's reverse pass on
-unseen scenarios and other K."""
+tests/golden/unrolled_ref.npz, and unrolled_warm_ref.npz for warm starts and
+frozen statuses) and against the oracle's reverse pass on unseen scenarios,
+other K and per-scenario statuses."""
 import os
 import sys
 
@@ -22,13 +23,13 @@ from test_unrolled_oracle import unrolled_loss_adjoints  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def _gpu_run(s, net, inp, d, rh, ke, K, cuda):
+def _gpu_run(s, net, inp, d, rh, ke, K, cuda, **warm):
     from wdsgpu_b200.autodiff import solve_unrolled
     D = torch.tensor(d, device=cuda).requires_grad_(True)
     RH = torch.tensor(rh, device=cuda).requires_grad_(True)
     KE = torch.tensor(ke, device=cuda).requires_grad_(True)
     R = torch.tensor(np.asarray(net.r_hw, dtype=np.float64), device=cuda).requires_grad_(True)
-    out = solve_unrolled(s, D, RH, ke=KE, r_hw=R, K=K)
+    out = solve_unrolled(s, D, RH, ke=KE, r_hw=R, K=K, **warm)
     h, q, e = out["head_ft"], out["flow_cfs"], out["emitter_cfs"]
     sens = torch.as_tensor(np.asarray(inp["sensors"]), device=cuda)
     pl = torch.as_tensor(np.asarray(net.pump_link), device=cuda)
@@ -67,6 +68,53 @@ def test_unrolled_against_oracle(cuda, K):
     u = Unrolled(Model(net))
     oo, st = u.forward(d, rh, ke=ke, K=K)
     assert np.abs(o["head_ft"] - oo["head_ft"]).max() < 1e-4
+    gd, grh, gke, gr = u.backward(st, *unrolled_loss_adjoints(net, inp, oo)[:3])
+    junc = np.asarray(net.node_type) == 0
+    for G, R, cols in ((g["g_demand"], gd, junc), (g["g_res_head"], grh, ~junc),
+                       (g["g_ke"], gke, junc), (g["g_rhw"], gr.sum(0), slice(None))):
+        assert np.abs(G[..., cols] - R[..., cols]).max() <= 1e-6 * np.abs(R[..., cols]).max()
+
+
+def test_unrolled_warm_matches_reference(cuda):
+    """Warm start q0 [B,L] / e0 [B,N] and frozen statuses [L] against the
+    reference's solve_unrolled (fixture unrolled_warm_ref.npz)."""
+    from wdsgpu_b200.solver import GGASolver
+    net, inp, ref = load("unrolled_warm_ref")
+    s = GGASolver(net, device=cuda, dense_status_machine=True)
+    o, g = _gpu_run(s, net, inp, inp["demand"], inp["res_head"], inp["ke"], int(inp["K"]), cuda,
+                    q0=torch.tensor(inp["q0"], device=cuda),
+                    e0=torch.tensor(inp["e0"], device=cuda), status=inp["status"])
+    assert np.abs(o["head_ft"] - ref["head"]).max() < 1e-4
+    assert np.abs(o["flow_cfs"] - ref["flow"]).max() < 1e-6
+    assert np.abs(o["emitter_cfs"] - ref["emitter"]).max() < 1e-6
+    junc = np.asarray(net.node_type) == 0
+    for key, cols in (("g_demand", junc), ("g_res_head", ~junc), ("g_ke", junc),
+                      ("g_rhw", slice(None))):
+        G, R = g[key][..., cols], ref[key][..., cols]
+        assert np.abs(G - R).max() <= 1e-6 * np.abs(R).max(), (key, np.abs(G - R).max())
+
+
+def test_unrolled_frozen_status_per_scenario(cuda):
+    """Per-scenario frozen statuses [B,L] without q0: the initial flows follow
+    the statuses (closed links QZERO); recording forward and reverse pass
+    against the oracle with the same start."""
+    from wdsgpu_b200 import synth
+    from wdsgpu_b200.solver import GGASolver
+    net, inp, _ = load("unrolled_warm_ref")
+    d, _ = synth.config2_scenarios(net, 4, seed=29, sigma=0.3)
+    rh = np.broadcast_to(np.nan_to_num(net.fixed_head_ft_at(0)), d.shape).copy()
+    ke = np.broadcast_to(np.asarray(net.node_ke, dtype=np.float64), d.shape).copy()
+    S = np.broadcast_to(np.asarray(inp["status"], dtype=np.int8), (4, net.L)).copy()
+    pipes = np.flatnonzero(np.asarray(net.link_type) == 1)
+    S[1, pipes[5]] = 2                      # another pipe closed in scenario 1
+    S[3, pipes[9]] = 2
+    s = GGASolver(net, device=cuda, dense_status_machine=True)
+    o, g = _gpu_run(s, net, inp, d, rh, ke, 7, cuda, status=S)
+    u = Unrolled(Model(net))
+    q0 = np.where(S <= 2, 1e-6, s._q_open)
+    oo, st = u.forward(d, rh, ke=ke, K=7, S=S, q0=q0)
+    assert np.abs(o["head_ft"] - oo["head_ft"]).max() < 1e-4
+    assert np.abs(o["flow_cfs"] - oo["flow_cfs"]).max() < 1e-6
     gd, grh, gke, gr = u.backward(st, *unrolled_loss_adjoints(net, inp, oo)[:3])
     junc = np.asarray(net.node_type) == 0
     for G, R, cols in ((g["g_demand"], gd, junc), (g["g_res_head"], grh, ~junc),

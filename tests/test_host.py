@@ -147,8 +147,8 @@ def test_pump_rows_host_rules():
 
 def test_unrolled_host_rules():
     """solve_unrolled refuses what the reference refuses (control valves) and
-    what this route does not take (warm starts, a frozen status, pump
-    parameters); the health probe checks its parameter name."""
+    what this route does not take (pump parameters); the health probe checks
+    its parameter name."""
     from wdsgpu_b200.autodiff import solve_unrolled, unrolled_grad_health
     s = GGASolver(synth.config2_network(), device="cpu", dense_status_machine=True)
     d, rh = s.net.demand_cfs_at(0), s.net.reservoir_head_ft_at(0)
@@ -156,7 +156,7 @@ def test_unrolled_host_rules():
         solve_unrolled(s, d, rh, K=3)
     s2 = GGASolver(synth.unrolled_network(), device="cpu", dense_status_machine=True)
     with pytest.raises(NotImplementedError):
-        solve_unrolled(s2, d, rh, K=3, status=np.zeros(s2.L, dtype=np.int8))
+        solve_unrolled(s2, d, rh, K=3, speed=s2.init_setting.copy())
     with pytest.raises(ValueError):
         solve_unrolled(s2, d, rh, K=3, assemble="dense")
     with pytest.raises(ValueError):

@@ -1,7 +1,9 @@
 """Unrolled-K pin: the oracle's K fixed GGA iterations and its explicit
 reverse pass against the reference's solve_unrolled and its autograd
 gradients (fixture tests/golden/unrolled_ref.npz, `make_golden.py
-unrolled`), plus central differences of the oracle's own K-iteration map."""
+unrolled`) and with a warm start and frozen statuses (unrolled_warm_ref.npz,
+`make_golden.py unrolled_warm`), plus central differences of the oracle's
+own K-iteration map."""
 import os
 import sys
 
@@ -79,3 +81,26 @@ def test_oracle_unrolled_central_difference():
         rm[k] -= eps
         fd = (loss(d, rp) - loss(d, rm)) / (2 * eps)
         assert abs(fd - gr[0, k]) <= 2e-3 * abs(gr[0, k]), (k, fd, gr[0, k])
+
+
+def test_oracle_unrolled_warm_matches_reference():
+    """Warm start q0 / e0 (the reference's own converged flows at 90 %
+    demand) and its final statuses frozen, K = 6."""
+    net, inp, ref = load("unrolled_warm_ref")
+    u = Unrolled(Model(net))
+    S = np.asarray(inp["status"], dtype=np.int8)
+    out, st = u.forward(inp["demand"], inp["res_head"], ke=inp["ke"], K=int(inp["K"]), S=S,
+                        q0=inp["q0"], e0=inp["e0"])
+    # the iterates of either code move by up to 1e-4 ft per iteration at the
+    # fixed point (the 1e8 penalty of the closed links amplifies the linear
+    # solves' rounding), so the state bars are those of the cold start
+    assert np.abs(out["head_ft"] - ref["head"]).max() < 1e-4
+    assert np.abs(out["flow_cfs"] - ref["flow"]).max() < 1e-6
+    assert np.abs(out["emitter_cfs"] - ref["emitter"]).max() < 1e-6
+    gd, grh, gke, gr = u.backward(st, *unrolled_loss_adjoints(net, inp, out)[:3])
+    junc = np.asarray(net.node_type) == 0
+    for g, key, cols in ((gd, "g_demand", junc), (grh, "g_res_head", ~junc), (gke, "g_ke", junc)):
+        R = ref[key][:, cols]
+        assert np.abs(g[:, cols] - R).max() <= 1e-6 * np.abs(R).max(), key
+    R = ref["g_rhw"]
+    assert np.abs(gr.sum(0) - R).max() <= 1e-6 * np.abs(R).max()

@@ -119,7 +119,7 @@ def load():
     lib.wds_adjoint_pumps.argtypes = [vp, ctypes.c_int32] + [vp] * 10 + [vp]
     lib.wds_adjoint_pumps.restype = ctypes.c_int
     lib.wds_unrolled_adjoint.argtypes = [vp, ctypes.c_int32, ctypes.c_int32] + [vp] * 4 + \
-        [ctypes.c_int64, vp, ctypes.c_int64] + [vp] * 8 + [vp]
+        [ctypes.c_int64, vp, ctypes.c_int64] + [vp] * 9 + [vp]
     lib.wds_unrolled_adjoint.restype = ctypes.c_int
     lib.wds_plan_stats.argtypes = [vp, c_int64_p]
     lib.wds_plan_stats.restype = ctypes.c_int

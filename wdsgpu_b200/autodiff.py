@@ -327,7 +327,7 @@ class UnrolledSM100(torch.autograd.Function):
     solve per iteration).  1-D inputs get the batch-summed gradient."""
 
     @staticmethod
-    def forward(ctx, demand, res_head, ke, r_hw, solver, K):
+    def forward(ctx, demand, res_head, ke, r_hw, solver, K, warm=None):
         s = solver
         dims = (demand.dim(), res_head.dim(), ke.dim(), r_hw.dim())
         devs = (demand.device, res_head.device, ke.device, r_hw.device)
@@ -335,14 +335,21 @@ class UnrolledSM100(torch.autograd.Function):
                                            ke.detach(), r_hw.detach())
         ke_t, r_t = ke_t.contiguous(), r_t.contiguous()
         rec = torch.empty(B, int(K), s.L + 2 * s.Nj, dtype=torch.float64, device=s.device)
+        q0, e0, S0 = warm if warm is not None else (None, None, None)
+        q0 = s._warm(q0, B, s.L)
+        e0 = s._warm(e0, B, s.N)
+        if S0 is not None:
+            S0 = torch.as_tensor(np.asarray(S0), dtype=torch.int8, device=s.device)
+            S0 = (S0.unsqueeze(0).expand(B, -1) if S0.dim() == 1 else S0).contiguous()
         o = s.run(d, rh, ke_t, r_t, B, int(K), 1e-12, False, -1, refine=2, refine_band=0.0,
-                  record=rec)
+                  record=rec, q0=q0, e0=e0, S0=S0)
         info = o["info"]
         if bool((info != 0).any()):
             bad = torch.nonzero(info != 0).flatten().tolist()
             raise RuntimeError("solve_unrolled: the node matrix of scenarios %s is not "
                                "positive definite%s" % (bad[:8], _not_pd_hint(s)))
         ctx.save_for_backward(d, rh, ke_t, r_t, rec)
+        ctx.S0 = S0
         ctx.solver, ctx.plan, ctx.B, ctx.K, ctx.dims, ctx.devs = s, o["plan"], B, int(K), dims, devs
         head, flow, emit, relerr = o["head"], o["flow"], o["emit"], o["relerr"]
         if all(x == 1 for x in dims[:3]):
@@ -374,7 +381,8 @@ class UnrolledSM100(torch.autograd.Function):
             p.handle, B, K, rec.data_ptr(), d.data_ptr(), rh.data_ptr(), ke_t.data_ptr(),
             0 if ke_t.shape[0] == 1 else N, r_t.data_ptr(), 0 if r_t.shape[0] == 1 else L,
             gH.data_ptr(), gQ.data_ptr(), gE.data_ptr(), gd.data_ptr(), grh.data_ptr(),
-            gke.data_ptr(), gr.data_ptr(), scr.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
+            gke.data_ptr(), gr.data_ptr(), scr.data_ptr(),
+            None if ctx.S0 is None else ctx.S0.data_ptr(), ctypes.c_void_p(cur.cuda_stream)),
             "wds_unrolled_adjoint")
         dm, dv = ctx.dims, ctx.devs
 
@@ -383,25 +391,28 @@ class UnrolledSM100(torch.autograd.Function):
             return g.sum(0) if dim == 1 else g
 
         return (_fit(gd, dm[0], dv[0]), _fit(grh, dm[1], dv[1]), _fit(gke, dm[2], dv[2]),
-                _fit(gr, dm[3] + 1, dv[3]), None, None)
+                _fit(gr, dm[3] + 1, dv[3]), None, None, None)
 
 
 def solve_unrolled(solver, demand, res_head, ke=None, r_hw=None, K=None, q0=None, e0=None,
                    speed=None, status=None, pump_h0=None, pump_r=None, assemble="csr",
                    linear_solver="sm100"):
-    """K fixed GGA iterations (no convergence test, the initial statuses),
-    differentiable w.r.t. demand, res_head, ke and r_hw through every
-    iteration (dgga/autodiff.py:1357-1664 contract).  Returns dict(head_ft,
+    """K fixed GGA iterations (no convergence test, statuses frozen: `status`,
+    internal codes [L] or [B,L], or the initial ones), from the warm start
+    q0 [L] or [B,L] / e0 [N] or [B,N] or the initial flows, differentiable
+    w.r.t. demand, res_head, ke and r_hw through every iteration
+    (dgga/autodiff.py:1357-1664 contract; the warm start is a constant, as
+    an input without requires_grad in the reference).  Returns dict(head_ft,
     flow_cfs, emitter_cfs, relerr).  Like the reference: CVPIPE/PIPE/PUMP/TCV
     networks only (control valves refused), K defaults to the network's
-    TRIALS.  Not taken on this route: q0/e0 warm starts, a frozen `status`,
-    pump parameters."""
+    TRIALS.  Not taken on this route: pump parameters (speed, pump_h0,
+    pump_r)."""
     if assemble != "csr" or linear_solver != "sm100":
         raise ValueError("the B200 route is assemble='csr', linear_solver='sm100'")
-    if any(x is not None for x in (q0, e0, speed, status, pump_h0, pump_r)):
+    if any(x is not None for x in (speed, pump_h0, pump_r)):
         raise NotImplementedError(
-            "solve_unrolled on the sm100 route starts from the initial flows and statuses "
-            "with the network's pump parameters (q0/e0/status/speed/pump_h0/pump_r refused)")
+            "solve_unrolled on the sm100 route runs with the network's pump parameters "
+            "(speed/pump_h0/pump_r refused; implicit_solve differentiates them)")
     s = solver
     lt = s._lt
     from .net import FCV as _FCV, PRV as _PRV, PSV as _PSV
@@ -416,7 +427,16 @@ def solve_unrolled(solver, demand, res_head, ke=None, r_hw=None, K=None, q0=None
     ke = s.node_ke_default if ke is None else ke
     r_hw = s.r_hw if r_hw is None else r_hw
     K = int(s.max_iter_default if K is None else K)
-    head, flow, emit, relerr = UnrolledSM100.apply(t(demand), t(res_head), t(ke), t(r_hw), s, K)
+    det = lambda x: None if x is None else (x.detach() if isinstance(x, torch.Tensor) else x)
+    if q0 is None and status is not None:
+        # initlinkflow under the frozen statuses (dgga/autodiff.py:1472-1485):
+        # closed links QZERO, the others as at set-up
+        st = np.asarray(det(status).cpu() if isinstance(status, torch.Tensor) else status)
+        q0 = np.where(st <= 2, 1e-6, s._q_open)
+    warm = (det(q0), det(e0), det(status)) if any(x is not None for x in (q0, e0, status)) \
+        else None
+    head, flow, emit, relerr = UnrolledSM100.apply(t(demand), t(res_head), t(ke), t(r_hw), s, K,
+                                                   warm)
     return dict(head_ft=head, flow_cfs=flow, emitter_cfs=emit, relerr=relerr)
 
 

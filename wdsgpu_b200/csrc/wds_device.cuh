@@ -2085,7 +2085,7 @@ __device__ __forceinline__ void unrolled_one(const DevNet& n, const DevWork& w, 
   double* dj = w.dj + (size_t)b * n.Nj;  // junction demands in elimination order
   for (int p = tid; p < n.Nj; p += NT) dj[p] = drow[n.jnode[p]];
   for (int f = tid; f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
-  for (int k = tid; k < n.L; k += NT) s.S[k] = n.status0[k];
+  for (int k = tid; k < n.L; k += NT) s.S[k] = u.s0 ? u.s0[(size_t)b * n.L + k] : n.status0[k];
   gsync<NT>();
   if (!build_emitters<NT>(n, s, kerow, 1)) return;  // uniform; the forward failed alike
   double* qb = u.scr + (size_t)b * (2 * n.L + 2 * n.Nj);

@@ -226,6 +226,7 @@ struct UnrollArgs {
   double* gke;          // [B][N]
   double* gr;           // [B][L]
   double* scr;          // [B][2 L + 2 Nj]
+  const int8_t* s0;     // [B][L] frozen statuses of the forward, or null (the network's)
 };
 int launch_unrolled(const DevNet& n, const DevWork& w, const UnrollArgs& u, int groups,
                     void* stream, std::string* err);

@@ -861,8 +861,6 @@ static int set_pump_opts(FwdArgs& a, const WdsForwardOpts* o, int L, const std::
   if (a.sflags && !o->status_machine)
     return fail(WDS_E_ARG, who + ": the schedule record needs status_machine 1");
   a.s0 = o->status0;
-  if (a.s0 && a.rec)
-    return fail(WDS_E_ARG, who + ": the unrolled mode starts from the network's statuses");
   if (a.rec && (o->status_machine || o->polish_steps >= 0))
     return fail(WDS_E_ARG, who + ": the unrolled mode runs with status_machine 0 and no polish");
   a.th_sp = o->pump_speed;
@@ -1046,7 +1044,7 @@ extern "C" int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K,
                                     int64_t ke_stride, const double* r, int64_t r_stride,
                                     const double* gH, const double* gQ, const double* gE,
                                     double* gd, double* grh, double* gke, double* gr,
-                                    double* scratch, void* stream) {
+                                    double* scratch, const int8_t* status0, void* stream) {
   using namespace wds;
   if (!plan || batch <= 0 || K <= 0 || !record || !demand || !fixed_head || !ke || !r || !gH ||
       !gQ || !gE || !gd || !grh || !gke || !gr || !scratch)
@@ -1061,7 +1059,7 @@ extern "C" int wds_unrolled_adjoint(WdsPlan* plan, int32_t batch, int32_t K,
   UnrollArgs u{};
   u.B = batch; u.K = K; u.rec = record; u.d = demand; u.rh = fixed_head; u.ke = ke;
   u.ke_stride = ke_stride; u.r = r; u.r_stride = r_stride; u.gH = gH; u.gQ = gQ; u.gE = gE;
-  u.gd = gd; u.grh = grh; u.gke = gke; u.gr = gr; u.scr = scratch;
+  u.gd = gd; u.grh = grh; u.gke = gke; u.gr = gr; u.scr = scratch; u.s0 = status0;
   std::string err;
   const int rc = launch_unrolled(plan->dn, plan->dw, u, plan->groups, stream, &err);
   plan->have_state = false;  // the reverse pass reuses the plan's factor workspace

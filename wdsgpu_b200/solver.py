@@ -416,6 +416,7 @@ class GGASolver:
         if pl.size:
             q = np.where(is_pump, K0 * pq0, q)
         q_init = np.where(st == 0, QZERO, q)
+        self._q_open = q          # initlinkflow of an open link (frozen-status warm starts)
         # custom pump curves, one range per link
         curve_ptr = np.zeros(L + 1, dtype=np.int32)
         cx, cy = [], []
