@@ -596,22 +596,36 @@ __device__ __forceinline__ void bwd_level(const TB& T, const FT* W, double* v, i
   }
 }
 
+// 2^-h with h = ceil(e / 2) for x = m 2^e (m in [1, 2)), so that x 2^-2h lies
+// in [0.5, 2); 1 for a diagonal that is not positive and finite (the pivot
+// check then reports it).  Scaling by it is exact.
+__device__ __forceinline__ double pow2_scale(double x) {
+  if (!(x > 0.0) || !isfinite(x)) return 1.0;
+  const long long e = ((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
+  const long long h = (e + 1) >> 1;
+  return __longlong_as_double((1023 - h) << 52);
+}
+
 // Inverse of the top block's Schur complement S (nT x nT, nT <= WDS_TOP_MAX)
 // by symmetric sweeps (Gauss-Jordan elimination without pivoting, in column
 // order; every pivot is then a pivot of the LDL^T of S, so its sign is the
-// positive-definiteness check):
-// sweeping k maps a_kk -> -1/p, a_ik -> a_ik/p, a_kj -> a_kj/p and
-// a_ij -> a_ij - (a_ik/p) a_kj (p = a_kk); after all nT sweeps the matrix is
-// -S^{-1}.  Thread (r, c) of a 16 x 16 grid holds the entries
-// (r + 16 a, c + 16 b), a, b < 3, of the full matrix in registers for all
-// sweeps, so that a sweep is one short run of instructions per thread (the
-// rank-1 update is 9 FMAs; the sweeps are issue-bound when the SM's scenario
-// groups overlap).  Column k+1 after sweep k goes through shared memory: two
-// alternating buffers of 49 (the column, zero beyond nT, then 1/p of its
-// pivot, which the pivot's owner computes and checks) and one group barrier
-// per sweep.  Every entry takes the general update; the lanes owning column
-// k, then those owning row k, overwrite those entries (switches on the
-// uniform block index, so the registers are never indexed at run time).  S is
+// positive-definiteness check).  S is first scaled to S' = D S D with D the
+// power-of-two diagonal that brings diag(S') into [0.5, 2) (exact), so the
+// pivots p of S' are at most about 2, and S^{-1} = D S'^{-1} D.
+// Sweeping k maps a_kk -> -1/p, a_ik -> a_ik/p, a_kj -> a_kj/p and
+// a_ij -> a_ij - (a_ik/p) a_kj; after all nT sweeps the matrix is -S'^{-1}.
+// With the pivot's entry of the published column set to p - 1, the one
+// rank-1 update a_ij -> a_ij - (c_i/p) c_j (c = column k) gives row and
+// column k as well: c_i - (c_i/p)(p - 1) = c_i/p, without cancellation since
+// |p - 1| <= 1 after the scaling; only a_kk is then overwritten (-1/p).
+// Thread (r, c) of a 16 x 16 grid holds the entries (r + 16 a, c + 16 b),
+// a, b < 3, of the full matrix in registers for all sweeps, so that a sweep
+// is 6 shared loads, 3 multiplies and 9 FMAs per thread (the sweeps are
+// issue-bound when the SM's scenario groups overlap).  Column k+1 after
+// sweep k goes through shared memory: two alternating buffers of 49 (the
+// column, then 1/p of its pivot, which the pivot's owner computes and
+// checks) and one group barrier per sweep; the register blocks are selected
+// by the uniform block index, so they are never indexed at run time.  S is
 // read from the factor slots listed in dslot, S^{-1} is written to Mg
 // (row-major, each entry by its owner).  Returns 1 when this thread owned a
 // pivot that was not positive and finite.  Runs as a separate function so
@@ -637,9 +651,25 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
       }
       a[ia][jb] = x;
     }
-  // both buffers zero (rows beyond nT stay zero), then column 0 and 1/p of its pivot
-  if (tid < 2 * ST) tb[tid] = 0.0;
+  // the scale of row i goes through tb[ST + i] (the diagonal's owner writes it)
+  if (r == c) {
+#pragma unroll
+    for (int ia = 0; ia < 3; ++ia)
+      if (r + 16 * ia < nT) tb[ST + r + 16 * ia] = pow2_scale(a[ia][ia]);
+  }
   gsync<NT>();
+  double dr[3], dc[3];
+#pragma unroll
+  for (int ia = 0; ia < 3; ++ia) {
+    dr[ia] = r + 16 * ia < nT ? tb[ST + r + 16 * ia] : 1.0;
+    dc[ia] = c + 16 * ia < nT ? tb[ST + c + 16 * ia] : 1.0;
+  }
+#pragma unroll
+  for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+    for (int jb = 0; jb < 3; ++jb) a[ia][jb] *= dr[ia] * dc[jb];
+  gsync<NT>();
+  // column 0 (rows beyond nT are zero), then p - 1 at the pivot and 1/p
   if (c == 0) {
 #pragma unroll
     for (int ia = 0; ia < 3; ++ia) tb[r + 16 * ia] = a[ia][0];
@@ -647,6 +677,7 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
       const double p = a[0][0];
       if (!(p > 0.0) || !isfinite(p)) bad = 1;
       tb[WDS_TOP_MAX] = __drcp_rn(p);
+      tb[0] = p - 1.0;
     }
   }
   gsync<NT>();
@@ -656,35 +687,32 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
     double* nb = tb + ((k + 1) & 1) * ST;
     const double ip = cb[WDS_TOP_MAX];
     const double c0 = cb[c], c1 = cb[c + 16], c2 = cb[c + 32];
-    const int km = k & 15, kb = k >> 4;
-    // general update; column k (a_ik = a_ik / p) where this lane owns it
-    const bool k0 = c == km && kb == 0, k1 = c == km && kb == 1, k2 = c == km && kb == 2;
 #pragma unroll
     for (int ia = 0; ia < 3; ++ia) {
       const double t = cb[r + 16 * ia] * ip;
-      a[ia][0] = k0 ? t : fma(-t, c0, a[ia][0]);
-      a[ia][1] = k1 ? t : fma(-t, c1, a[ia][1]);
-      a[ia][2] = k2 ? t : fma(-t, c2, a[ia][2]);
+      a[ia][0] = fma(-t, c0, a[ia][0]);
+      a[ia][1] = fma(-t, c1, a[ia][1]);
+      a[ia][2] = fma(-t, c2, a[ia][2]);
     }
-    if (r == km) {  // row k: a_kj = a_kj / p, and a_kk = -1/p
-      const double r0 = k0 ? -ip : c0 * ip;
-      const double r1 = k1 ? -ip : c1 * ip;
-      const double r2 = k2 ? -ip : c2 * ip;
-      if (kb == 0) {
-        a[0][0] = r0; a[0][1] = r1; a[0][2] = r2;
-      } else if (kb == 1) {
-        a[1][0] = r0; a[1][1] = r1; a[1][2] = r2;
-      } else {
-        a[2][0] = r0; a[2][1] = r1; a[2][2] = r2;
-      }
+    const int km = k & 15, kb = k >> 4;
+    if (r == km && c == km) {  // the pivot: a_kk = -1/p
+      if (kb == 0) a[0][0] = -ip;
+      else if (kb == 1) a[1][1] = -ip;
+      else a[2][2] = -ip;
     }
-    // publish column kn = k + 1 (all rows: the full matrix is kept) and 1/p
+    // publish column kn = k + 1 (all rows: the full matrix is kept), then
+    // p - 1 at its pivot and 1/p
     const int kn = k + 1;
     if (kn < nT && c == (kn & 15)) {
       const int nj = kn >> 4;
-      const double v0 = nj == 0 ? a[0][0] : (nj == 1 ? a[0][1] : a[0][2]);
-      const double v1 = nj == 0 ? a[1][0] : (nj == 1 ? a[1][1] : a[1][2]);
-      const double v2 = nj == 0 ? a[2][0] : (nj == 1 ? a[2][1] : a[2][2]);
+      double v0, v1, v2;
+      if (nj == 0) {
+        v0 = a[0][0]; v1 = a[1][0]; v2 = a[2][0];
+      } else if (nj == 1) {
+        v0 = a[0][1]; v1 = a[1][1]; v2 = a[2][1];
+      } else {
+        v0 = a[0][2]; v1 = a[1][2]; v2 = a[2][2];
+      }
       nb[r] = v0;
       nb[r + 16] = v1;
       nb[r + 32] = v2;
@@ -692,6 +720,7 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
         const double x = nj == 0 ? v0 : (nj == 1 ? v1 : v2);
         if (!(x > 0.0) || !isfinite(x)) bad = 1;
         nb[WDS_TOP_MAX] = __drcp_rn(x);
+        nb[kn] = x - 1.0;
       }
     }
     gsync<NT>();
@@ -701,7 +730,7 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
 #pragma unroll
     for (int jb = 0; jb < 3; ++jb) {
       const int i = r + 16 * ia, j = c + 16 * jb;
-      if (i < nT && j < nT) Mg[i * nT + j] = -a[ia][jb];
+      if (i < nT && j < nT) Mg[i * nT + j] = -a[ia][jb] * (dr[ia] * dc[jb]);
     }
   return bad;
 }
