@@ -73,7 +73,8 @@ enum {
 enum {
   WDS_INFO_NOT_PD = 1,      /* a pivot of the LDL^T factor was <= 0 or not finite */
   WDS_INFO_UNCONVERGED = 2, /* GGA loop ran out of trials                         */
-  WDS_INFO_EMITTER_CAP = 4  /* more emitters than the plan's emitter capacity     */
+  WDS_INFO_EMITTER_CAP = 4, /* more emitters than the plan's emitter capacity     */
+  WDS_INFO_BAD_HEAD = 8     /* a reservoir/tank head was NaN; nothing was solved */
 };
 
 /* Static network description (host pointers; copied by wds_plan). */

@@ -78,3 +78,32 @@ def test_graph_freed_without_backward_releases_the_plan(cuda):
     with torch.no_grad():
         implicit_solve(s, D, torch.tensor(rh, device=cuda), accuracy=1e-8)
     assert not any(p.held for p in s._plans) and len(s._plans) == 1
+
+
+def test_nan_reservoir_head_is_refused_and_the_solver_stays_usable(cuda):
+    """A NaN head at a reservoir/tank node raises ValueError (as the reference
+    does before its solve, dgga/solver.py:2892-2894); the forward kernel
+    reports it per scenario and solves nothing for it, and the next call on
+    the same solver is unaffected."""
+    from wdsgpu_b200.autodiff import solve_unrolled
+    net = synth.config2_network()
+    s = GGASolver(net, device=cuda, dense_status_machine=True)
+    d, rh = synth.config2_scenarios(net, 4, seed=77)
+    fixed = np.flatnonzero(np.asarray(net.node_type) != 0)
+    bad = rh.copy()
+    bad[2, fixed[0]] = np.nan
+    ref = s.solve(d, rh, status_machine=True, accuracy=1e-8)
+    with pytest.raises(ValueError, match="nan at a reservoir"):
+        s.solve(d, bad, status_machine=True, accuracy=1e-8)
+    with pytest.raises(ValueError, match="nan at a reservoir"):
+        implicit_solve(s, torch.tensor(d, device=cuda, requires_grad=True),
+                       torch.tensor(bad, device=cuda), accuracy=1e-8)
+    s2 = GGASolver(synth.unrolled_network(), device=cuda, dense_status_machine=True)
+    d2, rh2 = synth.config2_scenarios(s2.net, 2, seed=78)
+    rh2 = np.nan_to_num(rh2)
+    fx2 = np.flatnonzero(np.asarray(s2.net.node_type) != 0)
+    rh2[1, fx2[0]] = np.nan
+    with pytest.raises(ValueError, match="nan at a reservoir"):
+        solve_unrolled(s2, torch.tensor(d2, device=cuda), torch.tensor(rh2, device=cuda), K=4)
+    again = s.solve(d, rh, status_machine=True, accuracy=1e-8)
+    assert torch.equal(again["head_ft"], ref["head_ft"])

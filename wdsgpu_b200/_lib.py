@@ -18,7 +18,7 @@ c_double_p = ctypes.POINTER(ctypes.c_double)
 KIND_PIPE, KIND_CVPIPE, KIND_TCV, KIND_PUMP, KIND_PRV_FIXED, KIND_PRV, KIND_FCV, KIND_PSV = range(8)
 F_ZERO_SPEED, F_PUMP_LIVE, F_CHP, F_IS_PIPE = 1, 2, 4, 8
 TL_OVERFLOW, TL_IS_PUMP, TL_PUMP_IN, TL_PUMP_OUT = 1, 2, 4, 8
-INFO_NOT_PD, INFO_UNCONVERGED, INFO_EMITTER_CAP = 1, 2, 4
+INFO_NOT_PD, INFO_UNCONVERGED, INFO_EMITTER_CAP, INFO_BAD_HEAD = 1, 2, 4, 8
 LAYOUT_AUTO, LAYOUT_SHARED, LAYOUT_GLOBAL = 0, 1, 2
 E_NAMES = {-1: "bad argument", -2: "CUDA error", -3: "out of memory",
            -4: "unsupported network", -5: "no forward state"}

@@ -196,8 +196,8 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
                   pumps=pumps)
         info = o["info"]
         if bool((info != 0).any()):   # one host sync when every scenario converged
-            from .solver import _check_emitter_cap
-            _check_emitter_cap(s, info)
+            from .solver import _check_info_flags
+            _check_info_flags(s, info)
             bad = torch.nonzero(info != 0).flatten().tolist()
             np_ = torch.nonzero(info & _lib.INFO_NOT_PD).flatten().tolist()
             if np_:
@@ -345,6 +345,8 @@ class UnrolledSM100(torch.autograd.Function):
                   record=rec, q0=q0, e0=e0, S0=S0)
         info = o["info"]
         if bool((info != 0).any()):
+            from .solver import _check_info_flags
+            _check_info_flags(s, info)
             bad = torch.nonzero(info != 0).flatten().tolist()
             raise RuntimeError("solve_unrolled: the node matrix of scenarios %s is not "
                                "positive definite%s" % (bad[:8], _not_pd_hint(s)))

@@ -862,14 +862,24 @@ __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
 }
 
 // x = A^{-1} rhs with `refine` refinement steps against the matrix-free A.
-// unit >= 0 means rhs = e_unit.
+// unit >= 0 means rhs = e_unit.  An unrefined solve whose x lies outside
+// shared memory (the Woodbury columns and refinement corrections in the
+// global workspace) runs in the shared temporary t and stores x once, so
+// that its substitution levels chain on shared-memory latency.
 template <int NT, class FT, class TB>
 __device__ void solve_refined(const DevNet& n, const TB& T, const Sh& s, const double* rhs,
                               int unit, double* x, double* t, int refine) {
   const int tid = gtid<NT>();
-  for (int p = tid; p < n.Nj; p += NT) x[p] = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
+  const bool via_t = refine == 0 && t != nullptr && !__isShared(x) && __isShared(t);
+  double* v = via_t ? t : x;
+  for (int p = tid; p < n.Nj; p += NT) v[p] = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
   gsync<NT>();
-  solve<NT, FT>(n, T, s, x);
+  solve<NT, FT>(n, T, s, v);
+  if (via_t) {
+    for (int p = tid; p < n.Nj; p += NT) x[p] = v[p];
+    gsync<NT>();
+    return;
+  }
   for (int it = 0; it < refine; ++it) {
     for (int p = tid; p < n.Nj; p += NT) {
       const double b = unit >= 0 ? (p == unit ? 1.0 : 0.0) : rhs[p];
@@ -1394,13 +1404,18 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
   // read coalesced by every assembly
   double* dj = w.dj + (size_t)b * n.Nj;
   for (int p = gtid<NT>(); p < n.Nj; p += NT) dj[p] = drow[n.jnode[p]];
-  for (int f = gtid<NT>(); f < n.Nf; f += NT) s.hf[f] = rhrow[n.fnode[f]];
+  bool hf_nan = false;  // a reservoir/tank head that is NaN: nothing is solved
+  for (int f = gtid<NT>(); f < n.Nf; f += NT) {
+    const double h = rhrow[n.fnode[f]];
+    hf_nan = hf_nan || isnan(h);
+    s.hf[f] = h;
+  }
   for (int k = gtid<NT>(); k < n.L; k += NT) {
     s.q[k] = a.q0 ? a.q0[(size_t)b * n.L + k] : n.q_init[k];
     s.S[k] = a.s0 ? a.s0[(size_t)b * n.L + k] : n.status0[k];
   }
-  gsync<NT>();
-  const bool em_ok = build_emitters<NT>(n, s, kerow, 1);
+  hf_nan = gsync_or<NT>(hf_nan);
+  const bool em_ok = build_emitters<NT>(n, s, kerow, 1) && !hf_nan;
   if (a.e0) {  // warm start of the emitter flows (solver.py:2881-2887)
     for (int p = gtid<NT>(); p < n.Nj; p += NT) {
       const int es = s.eslot[p];
@@ -1754,7 +1769,8 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     gsync<NT>();
   }
   gsync<NT>();
-  if (!em_ok) info = WDS_INFO_EMITTER_CAP;
+  if (hf_nan) info = WDS_INFO_BAD_HEAD;
+  else if (!em_ok) info = WDS_INFO_EMITTER_CAP;
   if (gtid<NT>() == 0) w.valid[b] = (a.polish >= 0 && info == 0) ? 1 : 0;
   // ---- outputs
   double* hrow = a.head + (size_t)b * n.N;

@@ -45,7 +45,7 @@ import torch
 
 from . import _lib
 from .autodiff import _adjoint_guards, _clamp_grh, _clamp_rhs
-from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
+from .solver import GGASolver, _check_info_flags, _not_pd_hint
 
 __all__ = ["eps_solve", "EpsSM100", "tank_links"]
 
@@ -108,7 +108,7 @@ class _Tanks:
 def _step_forward(s, d, rh, ke, r, B, max_iter, acc, polish, q0, e0, S0=None):
     o = s.run(d, rh, ke, r, B, max_iter, acc, True, polish, q0=q0, e0=e0, S0=S0)
     info = o["info"]
-    _check_emitter_cap(s, info)
+    _check_info_flags(s, info)
     if bool((info != 0).any()):
         bad = torch.nonzero(info != 0).flatten().tolist()
         if bool((info & _lib.INFO_NOT_PD).any()):

@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from .autodiff import _adjoint_guards, _clamp_grh, _clamp_rhs
-from .solver import GGASolver, _Hold, _check_emitter_cap, _not_pd_hint
+from .solver import GGASolver, _Hold, _check_info_flags, _not_pd_hint
 
 __all__ = ["implicit_solve_multi", "solve_multi"]
 
@@ -94,7 +94,7 @@ def solve_multi(solvers, demands, res_heads, kes=None, r_hws=None, accuracy=None
     res = []
     for s, o in zip(solvers, outs):
         info = o["info"]
-        _check_emitter_cap(s, info)
+        _check_info_flags(s, info)
         bad = torch.nonzero(info & _lib.INFO_NOT_PD).flatten()
         if bad.numel():
             raise RuntimeError("batched LDL^T failed: the node matrix of scenarios %s is not "
@@ -122,7 +122,7 @@ class ImplicitMultiSM100(torch.autograd.Function):
         res, clamps = [], []
         for s, o in zip(solvers, outs):
             info = o["info"]
-            _check_emitter_cap(s, info)
+            _check_info_flags(s, info)
             if bool((info != 0).any()):
                 bad = torch.nonzero(info != 0).flatten().tolist()
                 if bool((info & _lib.INFO_NOT_PD).any()):

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .solver import GGASolver, _check_emitter_cap, _not_pd_hint
+from .solver import GGASolver, _check_info_flags, _not_pd_hint
 
 __all__ = ["sensitivity_matrix", "dr_dC_chain"]
 
@@ -66,7 +66,7 @@ def sensitivity_matrix(solver, demand, res_head, r_hw, sensor_nodes, wrt="C", fr
     o = s.run(d, rh, ke_t.contiguous(), r_t.contiguous(), B, int(max_iter), float(accuracy),
               True, int(polish_steps), pumps=pumps)
     info_v = o["info"]
-    _check_emitter_cap(s, info_v)
+    _check_info_flags(s, info_v)
     if bool((info_v != 0).any()):
         badb = torch.nonzero(info_v != 0).flatten().tolist()
         if bool((info_v & _lib.INFO_NOT_PD).any()):

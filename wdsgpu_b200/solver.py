@@ -174,7 +174,12 @@ def _not_pd_hint(solver):
     return ""
 
 
-def _check_emitter_cap(solver, info):
+def _check_info_flags(solver, info):
+    """Input errors the forward kernel reports per scenario: a NaN head at a
+    reservoir/tank node (dgga/solver.py:2892-2894; the kernel solves nothing
+    for that scenario) and more emitters than the plan's capacity."""
+    if bool((info & _lib.INFO_BAD_HEAD).any()):
+        raise ValueError("res_head_ft is nan at a reservoir/tank node")
     cap = torch.nonzero(info & _lib.INFO_EMITTER_CAP).flatten()
     if cap.numel():
         raise ValueError(
@@ -271,7 +276,6 @@ class GGASolver:
         is_junc = nt == 0
         self.junc_nodes = np.flatnonzero(is_junc)
         self.fixed_nodes = np.flatnonzero(~is_junc)
-        self._fixed_dev = None
         self.Nj = int(is_junc.sum())
         self.hexp = 1.852 if self.headloss_form == "H-W" else 2.0
         self.qexp = float(meta["qexp"])
@@ -548,10 +552,9 @@ class GGASolver:
         rh = rh.contiguous()
         ke = ke.contiguous()
         r = r.contiguous()
-        if self._fixed_dev is None:   # device copy of the reservoir/tank node index, once
-            self._fixed_dev = torch.as_tensor(self.fixed_nodes, device=self.device)
-        if torch.isnan(rh.index_select(1, self._fixed_dev)).any():
-            raise ValueError("res_head_ft is nan at a reservoir/tank node")
+        # a NaN reservoir/tank head is reported by the forward kernel (info
+        # WDS_INFO_BAD_HEAD, raised by _check_info_flags), so that the inputs
+        # cost no host synchronisation before the launch
         return d, rh, ke, r, B, single
 
     def _guards(self, status_machine, assemble, linear_solver, link_status,
@@ -758,7 +761,7 @@ class GGASolver:
         o = self.run(d, rh, ke, r, B, max_iter, hacc, sm, -1, q0=q0, e0=e0,
                      schedule=bool(record_schedule))
         info = o["info"]
-        _check_emitter_cap(self, info)
+        _check_info_flags(self, info)
         bad = torch.nonzero(info & _lib.INFO_NOT_PD).flatten()
         if bad.numel():
             raise RuntimeError(
