@@ -42,6 +42,9 @@ namespace wds {
 namespace {
 
 constexpr double kINF = __builtin_huge_val();
+// A polish step keeps its predecessor's factor when the predecessor moved the
+// flows by at most this fraction (sum |dq| / sum |q|).
+constexpr double kPolishReuse = 1e-4;
 
 struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
@@ -1159,7 +1162,7 @@ __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const
 template <int NT, class FT, class TB>
 __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* rp, double* dH,
                              double* res, double* sx, double* cols, const double* rprv,
-                             bool any_act, int outer) {
+                             bool any_act, int outer, bool cols_ready) {
   const double* rhs = s.V0;
   double* t = s.V2;
   const int tid = gtid<NT>();
@@ -1190,7 +1193,9 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
   gsync<NT>();
   // the outer refinement below contracts the error of these unrefined solves
   solve_refined<NT, FT>(n, T, s, rp, -1, dH, t, 0);
-  for (int c = 0; c < p; ++c) {  // X_c = A^{-1} sgn_c (e_jc - e_jo); zero for inactive valves
+  // the columns and C depend on the factor alone: a step that reuses the
+  // previous step's factor reuses them too (cols_ready)
+  for (int c = 0; c < (cols_ready ? 0 : p); ++c) {  // X_c = A^{-1} sgn_c (e_jc - e_jo); zero for inactive valves
     double* xc = cols + (size_t)c * n.Nj;
     if (actf[c] == 0.0) {
       for (int q = tid; q < n.Nj; q += NT) xc[q] = 0.0;
@@ -1206,7 +1211,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
     gsync<NT>();
     solve_refined<NT, FT>(n, T, s, res, -1, xc, t, 0);
   }
-  if (tid == 0)
+  if (tid == 0 && !cols_ready)
     for (int a0 = 0; a0 < p; ++a0)
       for (int c = 0; c < p; ++c)
         C[a0 * p + c] = actf[a0] != 0.0 ? cols[(size_t)c * n.Nj + n.pcv_jc[a0]]
@@ -1667,12 +1672,22 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     double* cols = sx + n.Nj;                          // 2p Woodbury columns
     // small buffer: C [4p^2], y [2p], actf [p], row1 [p], then r_prv [p]
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
+    // A step whose predecessor moved the flows by less than kPolishReuse
+    // (sum |dq| / sum |q|) keeps the predecessor's factor and Woodbury
+    // columns: the Jacobian has then changed by about that fraction, so the
+    // step's correction is exact to that fraction of itself and the next
+    // step contracts the rest; the last step's two outer refinements run
+    // against the current operator, and the terminal factor kept for the
+    // adjoint is always fresh.
+    bool reuse = false;
     for (int step = 0; step <= a.polish; ++step) {
       adj_coeffs<NT>(n, th, s, rrow, kerow);
-      assemble_reduced<NT, FT>(n, T, s);
-      if (!factor<NT, FT>(n, T, s)) {
-        info = WDS_INFO_NOT_PD;
-        break;
+      if (!reuse) {
+        assemble_reduced<NT, FT>(n, T, s);
+        if (!factor<NT, FT>(n, T, s)) {
+          info = WDS_INFO_NOT_PD;
+          break;
+        }
       }
       if (step == a.polish) break;  // terminal factor: keep it
       // residuals (autodiff.py:1032-1050); r_l overwrites Y
@@ -1716,15 +1731,19 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       // a Newton step corrects the rounding of the step before it: only the
       // last polish step's solve sets the final state, so it alone refines
       primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act,
-                           step == a.polish - 1 ? 2 : 0);
+                           step == a.polish - 1 ? 2 : 0, reuse);
       // dq, de, state update
+      double mv[2] = {0.0, 0.0};  // sum |dq|, sum |q|
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
         if (i >= 0 && s.S[k] == WDS_ACTIVE)  // the free valve flow, solved in slot jc
           dq = s.small[4 * n.npcv * n.npcv + 3 * n.npcv + i];
-        s.q[k] = s.q[k] + dq;
+        const double q2 = s.q[k] + dq;
+        s.q[k] = q2;
+        mv[0] += fabs(dq);
+        mv[1] += fabs(q2);
       }
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
         const int es = s.eslot[p];
@@ -1736,7 +1755,8 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
         }
         Hs[p] = Hs[p] + s.V1[p];
       }
-      gsync<NT>();
+      block_sum<NT>(mv, 2, s.red);  // its barriers publish the updates above
+      reuse = step + 1 < a.polish && mv[0] <= kPolishReuse * mv[1];
     }
     if (info == 0) {  // store the terminal state for the adjoint
       FT* Wt = reinterpret_cast<FT*>(w.W) + (size_t)b * n.nnzL;
