@@ -1677,8 +1677,11 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     // columns: the Jacobian has then changed by about that fraction, so the
     // step's correction is exact to that fraction of itself and the next
     // step contracts the rest; the last step's two outer refinements run
-    // against the current operator, and the terminal factor kept for the
-    // adjoint is always fresh.
+    // against the current operator.  The same holds for the terminal
+    // factor kept for the adjoint: every adjoint solve takes two refinement
+    // steps against the terminal operator (the coefficients stored with the
+    // state), which contract the factor's distance from it by that fraction
+    // each.
     bool reuse = false;
     for (int step = 0; step <= a.polish; ++step) {
       adj_coeffs<NT>(n, th, s, rrow, kerow);
@@ -1756,7 +1759,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
         Hs[p] = Hs[p] + s.V1[p];
       }
       block_sum<NT>(mv, 2, s.red);  // its barriers publish the updates above
-      reuse = step + 1 < a.polish && mv[0] <= kPolishReuse * mv[1];
+      reuse = mv[0] <= kPolishReuse * mv[1];
     }
     if (info == 0) {  // store the terminal state for the adjoint
       FT* Wt = reinterpret_cast<FT*>(w.W) + (size_t)b * n.nnzL;
