@@ -158,6 +158,15 @@ __device__ __forceinline__ double junc_of(int c, const double* x) { return c >= 
 // A group synchronises with its own named barrier (id 1 + group index).
 template <int NT>
 __device__ __forceinline__ int gtid() { return threadIdx.x & (NT - 1); }
+// The warp of a group that runs the narrow levels: warp g mod 4 of group g,
+// so that the co-resident groups' narrow chains issue from different SM
+// sub-partitions (warp w of a CTA issues from sub-partition w mod 4).
+template <int NT>
+__device__ __forceinline__ bool in_narrow_warp() {
+  constexpr int kWarps = NT / 32;
+  const int g = (int)(threadIdx.x / NT) & 3;
+  return (gtid<NT>() >> 5) == (g < kWarps ? g : 0);
+}
 template <int NT>
 __device__ __forceinline__ void gsync() {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / NT)), "r"(NT) : "memory");
@@ -782,7 +791,7 @@ __device__ __noinline__ void top_apply(const double* Mg, double* vT, int nT) {
 template <int NT, class FT, class TB>
 __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
   const int tid = gtid<NT>(), lane = tid & 31;
-  const bool inw = tid < 32;
+  const bool inw = in_narrow_warp<NT>();
   bool bad = false, prev_wide = true;
   // a level's mode and slot range are static: the next level's are loaded
   // while this level runs, so that a level starts with its own work
@@ -824,7 +833,7 @@ __device__ bool factor(const DevNet& n, const TB& T, const Sh& s) {
 template <int NT, class FT, class TB>
 __device__ void solve(const DevNet& n, const TB& T, const Sh& s, double* v) {
   const int tid = gtid<NT>(), lane = tid & 31;
-  const bool inw = tid < 32;
+  const bool inw = in_narrow_warp<NT>();
   bool prev_wide = true;
   // each level's mode and column range come from registers loaded a level ahead
   int md_n = n.L0 > 0 ? T.mfwd[0] : 0, c1_n = n.L0 > 0 ? T.levptr[1] : 0;
