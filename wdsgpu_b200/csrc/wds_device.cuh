@@ -42,9 +42,12 @@ namespace wds {
 namespace {
 
 constexpr double kINF = __builtin_huge_val();
-// A polish step keeps its predecessor's factor when the predecessor moved the
-// flows by at most this fraction (sum |dq| / sum |q|).
-constexpr double kPolishReuse = 1e-4;
+// A polish step keeps the factor in use while every link conductance P and
+// emitter term of the step is within kReuseStep (relative) of the values it
+// was factored with; the terminal state kept for the adjoint, within
+// kReuseTerminal.
+constexpr double kReuseStep = 1e-3;
+constexpr double kReuseTerminal = 1e-4;
 
 struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
@@ -1136,22 +1139,35 @@ __device__ void assemble_reduced(const DevNet& n, const TB& T, const Sh& s) {
 
 // Coefficients at the current state for polish / terminal (autodiff.py:786-875):
 // P, Y per link; emh per junction.
+// With Pf / Ef (the P of every link and 1/hg of every emitter slot that the
+// factor in use was formed with), `far` reports whether any of them moved
+// by more than tol, relative; their loads are issued before the
+// coefficients are formed.
 template <int NT>
 __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const double* rrow,
-                           const double* kerow) {
+                           const double* kerow, const double* Pf = nullptr,
+                           const double* Ef = nullptr, double tol = 0.0,
+                           bool* far = nullptr) {
   const int tid = gtid<NT>();
+  bool fr = false;
   for (int k = tid; k < n.L; k += NT) {
+    const double p0 = Pf ? Pf[k] : 0.0;
     double P, Y;
     link_coef(n, th, k, s.q[k], s.S[k], rrow[k], true, P, Y);
     s.P[k] = P;
     s.Y[k] = Y;
+    if (Pf) fr = fr || !(fabs(P - p0) <= tol * fabs(p0));
   }
   const int nem = s.flag[2];
   for (int es = tid; es < nem; es += NT) {
+    const double e0 = Ef ? Ef[es] : 0.0;
     double hl, hg;
     emitter_hl(n, s.em_e[es], s.em_ke[es], hl, hg);
-    s.em_emh[es] = 1.0 / hg;
+    const double emh = 1.0 / hg;
+    s.em_emh[es] = emh;
+    if (Ef) fr = fr || !(fabs(emh - e0) <= tol * fabs(e0));
   }
+  if (far) *far = fr;
   gsync<NT>();
 }
 
@@ -1681,25 +1697,35 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     double* cols = sx + n.Nj;                          // 2p Woodbury columns
     // small buffer: C [4p^2], y [2p], actf [p], row1 [p], then r_prv [p]
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
-    // A step whose predecessor moved the flows by less than kPolishReuse
-    // (sum |dq| / sum |q|) keeps the predecessor's factor and Woodbury
-    // columns: the Jacobian has then changed by about that fraction, so the
-    // step's correction is exact to that fraction of itself and the next
-    // step contracts the rest; the last step's two outer refinements run
-    // against the current operator.  The same holds for the terminal
-    // factor kept for the adjoint: every adjoint solve takes two refinement
-    // steps against the terminal operator (the coefficients stored with the
-    // state), which contract the factor's distance from it by that fraction
-    // each.
-    bool reuse = false;
+    // Factor reuse: a step keeps the factor in use (and its Woodbury columns)
+    // while every link conductance P and emitter term 1/hg of the step is
+    // within kReuseStep, relative, of the values it was factored with (kept
+    // in the workspace's P / emh rows until the terminal store).  The
+    // Jacobian then differs from the factored one by at most that fraction
+    // in every entry, so a step's correction is exact to that fraction of
+    // itself and the next step contracts the rest; the last step's two
+    // outer refinements run against the current operator.  The terminal
+    // state kept for the adjoint reuses it within kReuseTerminal: every
+    // adjoint solve takes two refinement steps against the terminal
+    // operator, which leave the cube of that distance.
+    double* Pf = w.P + (size_t)b * n.L;     // P of each link and 1/hg of each
+    double* Ef = w.emh + (size_t)b * n.Nj;  // emitter slot of the factor in use
+    bool have = false, reuse = false;
     for (int step = 0; step <= a.polish; ++step) {
-      adj_coeffs<NT>(n, th, s, rrow, kerow);
+      bool far = false;
+      adj_coeffs<NT>(n, th, s, rrow, kerow, have ? Pf : nullptr, have ? Ef : nullptr,
+                     step == a.polish ? kReuseTerminal : kReuseStep, &far);
+      reuse = have && !gsync_or<NT>(far);
       if (!reuse) {
         assemble_reduced<NT, FT>(n, T, s);
         if (!factor<NT, FT>(n, T, s)) {
           info = WDS_INFO_NOT_PD;
           break;
         }
+        // each thread keeps the entries it compares (the same index mapping)
+        for (int k = gtid<NT>(); k < n.L; k += NT) Pf[k] = s.P[k];
+        for (int es = gtid<NT>(); es < s.flag[2]; es += NT) Ef[es] = s.em_emh[es];
+        have = true;
       }
       if (step == a.polish) break;  // terminal factor: keep it
       // residuals (autodiff.py:1032-1050); r_l overwrites Y
@@ -1745,17 +1771,13 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act,
                            step == a.polish - 1 ? 2 : 0, reuse);
       // dq, de, state update
-      double mv[2] = {0.0, 0.0};  // sum |dq|, sum |q|
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
         if (i >= 0 && s.S[k] == WDS_ACTIVE)  // the free valve flow, solved in slot jc
           dq = s.small[4 * n.npcv * n.npcv + 3 * n.npcv + i];
-        const double q2 = s.q[k] + dq;
-        s.q[k] = q2;
-        mv[0] += fabs(dq);
-        mv[1] += fabs(q2);
+        s.q[k] = s.q[k] + dq;
       }
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
         const int es = s.eslot[p];
@@ -1767,8 +1789,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
         }
         Hs[p] = Hs[p] + s.V1[p];
       }
-      block_sum<NT>(mv, 2, s.red);  // its barriers publish the updates above
-      reuse = mv[0] <= kPolishReuse * mv[1];
+      gsync<NT>();
     }
     if (info == 0) {  // store the terminal state for the adjoint
       FT* Wt = reinterpret_cast<FT*>(w.W) + (size_t)b * n.nnzL;
