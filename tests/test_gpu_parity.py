@@ -96,6 +96,31 @@ def test_config2_against_oracle_fresh_seed(cuda):
     assert _rel(_np(RH.grad), grh) < GRAD_RTOL
 
 
+@pytest.mark.parametrize("accuracy", [1e-2, 1e-4])
+def test_polish_factor_reuse_at_loose_accuracy(cuda, accuracy):
+    """A loose GGA accuracy moves the Jacobian between polish steps, so the
+    polish re-factors where needed and reuses a factor only within its
+    per-entry bound: polished heads, flows and gradients still agree with
+    the oracle's full Newton polish (which re-factors at every step)."""
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, 6, seed=321)
+    sens = synth.sensor_nodes(net, 30)
+    m = Model(net)
+    out, st = m.implicit(d, rh, accuracy=accuracy, polish_steps=3, status_machine=True)
+    gH = np.zeros_like(out["head_ft"])
+    gH[:, sens] = 2.0 * out["head_ft"][:, sens]
+    gd = m.backward(st, gH, np.zeros_like(out["flow_cfs"]), np.zeros_like(out["emitter_cfs"]))[0]
+    s = GGASolver(net, device=cuda, dense_status_machine=True)
+    D = torch.tensor(d, device=cuda, requires_grad=True)
+    h, q, e = implicit_solve(s, D, torch.tensor(rh, device=cuda), accuracy=accuracy,
+                             status_machine=True)
+    (h[:, sens] ** 2).sum().backward()
+    assert np.abs(_np(h) - out["head_ft"]).max() < POLISHED_HEAD_ATOL_FT
+    assert _rel(_np(D.grad), gd) < GRAD_RTOL
+    assert np.abs(_np(q) - out["flow_cfs"]).max() < POLISHED_FLOW_ATOL
+    assert np.abs(_np(e) - out["emitter_cfs"]).max() < POLISHED_FLOW_ATOL
+
+
 def test_batched_equals_single_bitwise(cuda):
     net = synth.config2_network()
     s = GGASolver(net, device=cuda, dense_status_machine=True)
