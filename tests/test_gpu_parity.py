@@ -117,8 +117,10 @@ def test_polish_factor_reuse_at_loose_accuracy(cuda, accuracy):
     (h[:, sens] ** 2).sum().backward()
     assert np.abs(_np(h) - out["head_ft"]).max() < POLISHED_HEAD_ATOL_FT
     assert _rel(_np(D.grad), gd) < GRAD_RTOL
-    assert np.abs(_np(q) - out["flow_cfs"]).max() < POLISHED_FLOW_ATOL
-    assert np.abs(_np(e) - out["emitter_cfs"]).max() < POLISHED_FLOW_ATOL
+    # three polish steps from a loose state leave both codes about 1e-10 of
+    # the flows away from the root, from raw states that differ by rounding
+    assert np.abs(_np(q) - out["flow_cfs"]).max() < 1e-9 * np.abs(out["flow_cfs"]).max()
+    assert np.abs(_np(e) - out["emitter_cfs"]).max() < 1e-9 * np.abs(out["flow_cfs"]).max()
 
 
 def test_batched_equals_single_bitwise(cuda):

@@ -48,6 +48,10 @@ constexpr double kINF = __builtin_huge_val();
 // kReuseTerminal.
 constexpr double kReuseStep = 1e-3;
 constexpr double kReuseTerminal = 1e-4;
+// ... and only once the previous step moved the flows by at most this
+// fraction (sum |dq| / sum |q|): the polish is then in its quadratic regime,
+// where a chord step equals the Newton step to rounding.
+constexpr double kReuseFlow = 1e-6;
 
 struct Sh {
   double *q, *P, *Y, *W, *V0, *V1, *V2, *hf, *xf, *red, *small;
@@ -1697,25 +1701,28 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     double* cols = sx + n.Nj;                          // 2p Woodbury columns
     // small buffer: C [4p^2], y [2p], actf [p], row1 [p], then r_prv [p]
     double* rprv = s.small + 4 * n.npcv * n.npcv + 4 * n.npcv;
-    // Factor reuse: a step keeps the factor in use (and its Woodbury columns)
+    // Factor reuse: once the previous step moved the flows by at most
+    // kReuseFlow, a step keeps the factor in use (and its Woodbury columns)
     // while every link conductance P and emitter term 1/hg of the step is
     // within kReuseStep, relative, of the values it was factored with (kept
     // in the workspace's P / emh rows until the terminal store).  The
     // Jacobian then differs from the factored one by at most that fraction
-    // in every entry, so a step's correction is exact to that fraction of
-    // itself and the next step contracts the rest; the last step's two
-    // outer refinements run against the current operator.  The terminal
-    // state kept for the adjoint reuses it within kReuseTerminal: every
-    // adjoint solve takes two refinement steps against the terminal
-    // operator, which leave the cube of that distance.
+    // in every entry, so the step's correction differs from the Newton
+    // correction by that fraction of itself, which in the quadratic regime
+    // is below rounding; the last step's two outer refinements run against
+    // the current operator.  The terminal state kept for the adjoint reuses
+    // it within kReuseTerminal: every adjoint solve takes two refinement
+    // steps against the terminal operator, which leave the cube of that
+    // distance.
     double* Pf = w.P + (size_t)b * n.L;     // P of each link and 1/hg of each
     double* Ef = w.emh + (size_t)b * n.Nj;  // emitter slot of the factor in use
-    bool have = false, reuse = false;
+    bool have = false, reuse = false, settled = false;
     for (int step = 0; step <= a.polish; ++step) {
       bool far = false;
-      adj_coeffs<NT>(n, th, s, rrow, kerow, have ? Pf : nullptr, have ? Ef : nullptr,
+      const bool cand = have && settled;
+      adj_coeffs<NT>(n, th, s, rrow, kerow, cand ? Pf : nullptr, cand ? Ef : nullptr,
                      step == a.polish ? kReuseTerminal : kReuseStep, &far);
-      reuse = have && !gsync_or<NT>(far);
+      reuse = cand && !gsync_or<NT>(far);
       if (!reuse) {
         assemble_reduced<NT, FT>(n, T, s);
         if (!factor<NT, FT>(n, T, s)) {
@@ -1771,13 +1778,17 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act,
                            step == a.polish - 1 ? 2 : 0, reuse);
       // dq, de, state update
+      double mv[2] = {0.0, 0.0};  // sum |dq|, sum |q|
       for (int k = gtid<NT>(); k < n.L; k += NT) {
         const double b1 = junc_of(T.e1[k], s.V1), b2 = junc_of(T.e2[k], s.V1);
         double dq = -s.P[k] * (s.Y[k] + (b2 - b1));
         const int i = n.link_pcv[k];
         if (i >= 0 && s.S[k] == WDS_ACTIVE)  // the free valve flow, solved in slot jc
           dq = s.small[4 * n.npcv * n.npcv + 3 * n.npcv + i];
-        s.q[k] = s.q[k] + dq;
+        const double q2 = s.q[k] + dq;
+        s.q[k] = q2;
+        mv[0] += fabs(dq);
+        mv[1] += fabs(q2);
       }
       for (int p = gtid<NT>(); p < n.Nj; p += NT) {
         const int es = s.eslot[p];
@@ -1789,7 +1800,8 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
         }
         Hs[p] = Hs[p] + s.V1[p];
       }
-      gsync<NT>();
+      block_sum<NT>(mv, 2, s.red);  // its barriers publish the updates above
+      settled = mv[0] <= kReuseFlow * mv[1];
     }
     if (info == 0) {  // store the terminal state for the adjoint
       FT* Wt = reinterpret_cast<FT*>(w.W) + (size_t)b * n.nnzL;
