@@ -47,8 +47,9 @@ def _adjoint_guards(s: GGASolver, flow, S, pumps=None, allow_clamp=False):
     (hydcoeffs.c:748-757) are refused unless allow_clamp; then the clamped
     entries are returned as (scenario, link, assembled P) tensors (None when
     there are none) for `_clamp_rhs`."""
-    if s.n_pcv:
+    if s.n_pcv and not getattr(s, "_pcv_guards_ok", False):
         # the junction each PRV (n2) or PSV (n1) holds, and its other end
+        # (static per network: checked once)
         jc, jo = s.pcv_jc, s.pcv_jo
         if np.unique(jc).size < jc.size:
             raise NotImplementedError(
@@ -57,6 +58,7 @@ def _adjoint_guards(s: GGASolver, flow, S, pumps=None, allow_clamp=False):
             raise NotImplementedError(
                 "adjoint='gpu': cascaded PRVs/PSVs (a held junction is another "
                 "valve's other end)")
+        s._pcv_guards_ok = True
     chp = s._tables["pump_type"] == 0
     if not chp.any():
         return None
@@ -233,8 +235,8 @@ class ImplicitGGASolveSM100(torch.autograd.Function):
         N, L = s.N, s.L
 
         def _g(g, n):
-            if g is None:
-                return torch.zeros(B, n, dtype=torch.float64, device=dev)
+            if g is None:   # a read-only input of the adjoint: one cached zero block
+                return s._zero_rows(B, n)
             g = g.detach().to(dtype=torch.float64, device=dev)
             g = g.unsqueeze(0).expand(B, -1) if g.dim() == 1 else g
             return g.contiguous()
@@ -368,8 +370,8 @@ class UnrolledSM100(torch.autograd.Function):
         dev, N, L = s.device, s.N, s.L
 
         def _g(g, n):
-            if g is None:
-                return torch.zeros(B, n, dtype=torch.float64, device=dev)
+            if g is None:   # a read-only input of the adjoint: one cached zero block
+                return s._zero_rows(B, n)
             g = g.detach().to(dtype=torch.float64, device=dev)
             return (g.unsqueeze(0).expand(B, -1) if g.dim() == 1 else g).contiguous()
 

@@ -294,6 +294,7 @@ class GGASolver:
                                                device=self.device)
         self.r_hw = torch.as_tensor(np.asarray(net.r_hw, dtype=np.float64), device=self.device)
         self._plans = []
+        self._zeros = {}
 
     # ------------------------------------------------------------ set-up
     @staticmethod
@@ -526,6 +527,17 @@ class GGASolver:
         return self.plan(1).symbolic()
 
     # ------------------------------------------------------------ solve
+    def _zero_rows(self, B, n):
+        """A cached [B, n] float64 block of zeros on the solver's device, for
+        read-only inputs of the C ABI (an output adjoint that autograd left
+        as None); never written."""
+        key = (int(B), int(n))
+        z = self._zeros.get(key)
+        if z is None:
+            z = torch.zeros(key, dtype=torch.float64, device=self.device)
+            self._zeros[key] = z
+        return z
+
     def _cvt(self, x):
         if isinstance(x, torch.Tensor):
             return x.to(dtype=torch.float64, device=self.device)
