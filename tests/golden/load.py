@@ -5,7 +5,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = ("cfg1", "cfg2", "feat_mid", "feat_low", "cfg3_small", "cfg3_tcv")
+CASES = ("cfg1", "cfg2", "cfg2_wide", "feat_mid", "feat_low", "cfg3_small", "cfg3_tcv")
 
 
 def load(tag):

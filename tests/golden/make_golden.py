@@ -26,6 +26,7 @@ Usage:  REFERENCE_ROOT=<dir> python tests/golden/make_golden.py   (steady cases)
                                                    and chp_ref.npz)
         python tests/golden/make_golden.py fcv    (flow control valve pin, fcv_ref.npz)
         python tests/golden/make_golden.py psv    (pressure sustaining valve pin, psv_ref.npz)
+        python tests/golden/make_golden.py cfg2_wide (config 2, 24 scenarios, cfg2_wide.npz)
         python tests/golden/make_golden.py unrolled (unrolled-K gradient pin, unrolled_ref.npz)
         python tests/golden/make_golden.py unrolled_warm (warm start and frozen statuses,
                                                    unrolled_warm_ref.npz)
@@ -186,6 +187,22 @@ def write_cases(dgga, torch, cases):
         print("%-9s iters=%s -> %s (%d KB)" % (
             tag, res["fwd_iters"].tolist(), os.path.basename(path),
             os.path.getsize(path) // 1024))
+
+
+def make_cfg2_wide():
+    """Config 2 at 24 scenarios with a wider demand spread (lognormal 0.35,
+    seed 12): more scenarios of the headline network, more PRV status
+    changes, pinned to the reference like cfg2."""
+    import torch
+    sys.path.insert(0, REPO)
+    from wdsgpu_b200 import synth
+    dgga = _load_reference()
+    torch.set_default_dtype(torch.float64)
+    net = synth.config2_network()
+    d, rh = synth.config2_scenarios(net, 24, seed=12, sigma=0.35)
+    ke = np.broadcast_to(net.node_ke, d.shape).copy()
+    sens = synth.sensor_nodes(net, 30)
+    write_cases(dgga, torch, {"cfg2_wide": (net, d, rh, ke, sens, 1e-6, True, False)})
 
 
 def make_cfg3():
@@ -635,6 +652,8 @@ if __name__ == "__main__":
         make_unrolled()
     elif sys.argv[1:] == ["unrolled_warm"]:
         make_unrolled_warm()
+    elif sys.argv[1:] == ["cfg2_wide"]:
+        make_cfg2_wide()
     elif sys.argv[1:] == ["cfg3"]:
         make_cfg3()
     elif sys.argv[1:] == ["valves"]:
