@@ -202,8 +202,9 @@ typedef struct WdsForwardOpts {
   /* Initial link statuses (WDS_XHEAD .. WDS_XPRESSURE), a device array
    * int8 [B][L], or NULL for the network's status0: the status warm start
    * of an extended-period step, which EpsDriver.run carries from frame to
-   * frame (run_gga(status0=S), dgga/eps.py:366-373).  Not with
-   * unroll_record. */
+   * frame (run_gga(status0=S), dgga/eps.py:366-373).  With unroll_record,
+   * the frozen statuses of solve_unrolled's `status` (pass the same array
+   * to wds_unrolled_adjoint). */
   const int8_t* status0;
 } WdsForwardOpts;
 
