@@ -166,8 +166,9 @@ def _oracle_scenarios(payload):
     return float(g[0].sum())
 
 
-def cpu_baseline_single(n_scen=3):
-    """The oracle port timed on one host core (the `cpu_baseline` object)."""
+def cpu_baseline_single(n_scen=36):
+    """The oracle port timed on one host core (the `cpu_baseline` object), on
+    a sample of about ten seconds of CPU work."""
     from wdsgpu_b200 import synth
     net = synth.config2_network()
     d, rh = synth.config2_scenarios(net, n_scen, seed=4242)
@@ -780,7 +781,7 @@ def main():
     # GGA iterations counted without refinement (the band refines only the
     # last one or two of them, so this is a lower bound); polish steps and
     # the terminal factor with two refinements
-    rg = s.refine_steps() if s.refine_band(ACCURACY) <= 0.0 else 0
+    rg = s.refine_steps(ACCURACY) if s.refine_band(ACCURACY) <= 0.0 else 0
     bpi = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"], refine=rg)
     bpi2 = bytes_per_iteration(net.L, st["nnz_A_lower"], st["nnz_L"], st["Nj"])
     fwd_bytes = float(iters.sum()) * bpi + B * (POLISH + 1) * bpi2

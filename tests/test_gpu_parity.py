@@ -255,20 +255,21 @@ def test_full_batch_config2_properties(cuda):
 
 
 def test_refine_band_keeps_iterations_and_statuses(cuda):
-    """The default schedule (GGA solves refined only once relerr < 1e-5, at
-    accuracy >= 1e-8) against the reference's schedule (every GGA solve
-    refined twice, refine_band = 0) on 256 unseen config-2 scenarios:
+    """The default schedule (GGA solves refined once, and only once relerr <
+    1e-5, at accuracy >= 1e-8) against the reference's schedule (every GGA
+    solve refined twice, refine_band = 0) on 256 unseen config-2 scenarios:
     identical iteration counts and statuses, polished state within 1e-9 m."""
     net = synth.config2_network()
     s = GGASolver(net, device=cuda, dense_status_machine=True)
     assert s.refine_band(1e-6) == 1e-5 and s.refine_band(1e-12) == 0.0
+    assert s.refine_steps(1e-6) == 1 and s.refine_steps(1e-12) == 2
     d, rh = synth.config2_scenarios(net, 256, seed=404)
     d = torch.tensor(d, device=cuda)
     rh = torch.tensor(rh, device=cuda)
     ke = s.node_ke_default.unsqueeze(0).contiguous()
     r = s.r_hw.unsqueeze(0).contiguous()
     a = s.run(d, rh, ke, r, 256, 200, 1e-6, True, 3)
-    b = s.run(d, rh, ke, r, 256, 200, 1e-6, True, 3, refine_band=0.0)
+    b = s.run(d, rh, ke, r, 256, 200, 1e-6, True, 3, refine=2, refine_band=0.0)
     assert int(a["info"].abs().sum()) == 0 and int(b["info"].abs().sum()) == 0
     assert torch.equal(a["iters"], b["iters"])
     assert torch.equal(a["status"], b["status"])

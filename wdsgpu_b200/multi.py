@@ -52,7 +52,7 @@ def _forward_multi(solvers, ins, accuracy, max_iter, status_machine, polish_step
         op.accuracy = float(accuracy)
         op.max_iter = int(max_iter)
         op.status_machine = 1 if status_machine else 0
-        op.refine = s.refine_steps()
+        op.refine = s.refine_steps(accuracy)
         op.refine_band = s.refine_band(accuracy)
         op.polish_steps = int(polish_steps)
         op.ke_stride = 0 if ke.shape[0] == 1 else s.N

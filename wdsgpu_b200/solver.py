@@ -201,8 +201,12 @@ class GGASolver:
     no damping, no HEADERROR/FLOWCHANGE, no junction-pressure controls, PRVs
     with a setting must join two junctions.
 
-    `sm100_refine` (default 2) is the number of iterative-refinement steps of
-    a refined GGA solve, mirroring `dense_refine` / `cudss_refine`.
+    `sm100_refine` is the number of iterative-refinement steps of a refined
+    GGA solve (the reference's `dense_refine` / `cudss_refine` are 2).  None
+    (default): 1 at accuracy >= 1e-8, where one step leaves the solve's
+    rounding at about (kappa u)^2, some 1e-14 relative at config 2, nine
+    orders below the convergence test; 2 at tighter accuracies, where the
+    convergence test sits at the rounding floor.
     `sm100_refine_band` says which GGA iterations refine: an iteration whose
     previous relerr is below the band (or past iteration 20) refines, the
     others take one unrefined FP64 substitution, whose rounding (about 1e-11
@@ -241,7 +245,7 @@ class GGASolver:
         self.device = torch.device(device)
         self.dtype = dtype
         self.net = net
-        self.sm100_refine = 2
+        self.sm100_refine = None
         self.sm100_refine_band = None
         self.sm100_layout = "auto"
         # schedule choices of the planner (groups_per_cta, top_max,
@@ -606,9 +610,12 @@ class GGASolver:
                 "record_schedule=True covers the batched status machine only "
                 "(status_machine=True), as in the reference")
 
-    def refine_steps(self):
-        """Refinement steps of a refined GGA solve (`sm100_refine`)."""
-        return int(self.sm100_refine)
+    def refine_steps(self, accuracy=None):
+        """Refinement steps of a refined GGA solve (`sm100_refine`; None: 1 at
+        accuracy >= 1e-8, else 2)."""
+        if self.sm100_refine is not None:
+            return int(self.sm100_refine)
+        return 1 if accuracy is not None and float(accuracy) >= 1e-8 else 2
 
     def refine_band(self, accuracy):
         """Refinement band of the GGA iterations (see `sm100_refine_band`)."""
@@ -677,7 +684,7 @@ class GGASolver:
         o.accuracy = float(hacc)
         o.max_iter = int(max_iter)
         o.status_machine = 1 if status_machine else 0
-        o.refine = int(self.refine_steps() if refine is None else refine)
+        o.refine = int(self.refine_steps(hacc) if refine is None else refine)
         o.refine_band = float(self.refine_band(hacc) if refine_band is None else refine_band)
         if record is not None:   # unrolled mode: max_iter iterations, recorded
             o.unroll_record = record.data_ptr()
