@@ -1183,8 +1183,8 @@ __device__ void adj_coeffs(const DevNet& n, const PumpTh& th, const Sh& s, const
 // flow in slot jc: M y = r', M = the factored A with column jc replaced by u
 // (the transpose of the adjoint's row-replaced matrix), r' = rhs - A_red[:,jc]
 // dH_jc.  Woodbury on the factor: A^{-1} u_a - e_jc (one solve per active
-// valve, right-hand side e_jc - e_jo), C_ab = X_b[jc_a], and two outer
-// refinement steps against the true M (`outer`, two on the last polish step)
+// valve, right-hand side e_jc - e_jo), C_ab = X_b[jc_a], and `outer`
+// refinement steps against the true M (one on the last polish step)
 // make the result independent of the unrefined inner solves.  Output: dH
 // (with dH_jc = -r_valve) and the valve flow corrections dqv[p].  rhs: V0
 // (kept).
@@ -1195,7 +1195,7 @@ __device__ void primal_solve(const DevNet& n, const TB& T, const Sh& s, double* 
   const double* rhs = s.V0;
   double* t = s.V2;
   const int tid = gtid<NT>();
-  if (!any_act) {  // `outer` refinement steps (two on the last polish step)
+  if (!any_act) {  // `outer` refinement steps (one on the last polish step)
     solve_refined<NT, FT>(n, T, s, rhs, -1, dH, t, outer);
     return;
   }
@@ -1709,7 +1709,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
     // Jacobian then differs from the factored one by at most that fraction
     // in every entry, so the step's correction differs from the Newton
     // correction by that fraction of itself, which in the quadratic regime
-    // is below rounding; the last step's two outer refinements run against
+    // is below rounding; the last step's outer refinement runs against
     // the current operator.  The terminal state kept for the adjoint reuses
     // it within kReuseTerminal: every adjoint solve takes two refinement
     // steps against the terminal operator, which leave the cube of that
@@ -1776,7 +1776,7 @@ __device__ __forceinline__ void forward_one(const DevNet& n, const DevWork& w, c
       // a Newton step corrects the rounding of the step before it: only the
       // last polish step's solve sets the final state, so it alone refines
       primal_solve<NT, FT>(n, T, s, rp, s.V1, res, sx, cols, rprv, any_act,
-                           step == a.polish - 1 ? 2 : 0, reuse);
+                           step == a.polish - 1 ? 1 : 0, reuse);
       // dq, de, state update
       double mv[2] = {0.0, 0.0};  // sum |dq|, sum |q|
       for (int k = gtid<NT>(); k < n.L; k += NT) {
